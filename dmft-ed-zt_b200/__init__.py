@@ -1,0 +1,315 @@
+"""B200 (sm_100a) zero-temperature ED impurity solver: Python host mirror.
+
+A thin ctypes front end over the C ABI in include/edzt.h (libedzt.so, built
+in this directory).  The classes and methods mirror the Fortran procedures
+of the reference (yw-choi/DMFT-ED-ZT) that the library replaces:
+
+  generate_basis      src/ed_basis.f90:42-114
+  hx                  src/impurity_hamiltonian.f90:77-247
+  apply_c             src/ed_operator.f90:13-57
+  lanczos_iteration   src/lanczos_solver.f90:92-173
+  diag_lanczos        src/lanczos_solver.f90:20-90
+  ground_state        src/ground_state.f90:1-81
+  green_diag          src/dmft_green.f90:177-260
+  cluster_green_ftn   src/dmft_green.f90:47-126
+
+Errors raise EDError carrying the library's status code (the reference
+aborts through die()).  There is no CPU fallback: if libedzt.so or a CUDA
+device is missing, constructing a Solver raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libedzt.so")
+REPO_ROOT = os.path.dirname(PKG_DIR)
+
+EDZT_OK = 0
+EDZT_ERR_ARG = 1
+EDZT_ERR_CUDA = 2
+EDZT_ERR_OOM = 3
+EDZT_ERR_STATE = 4
+EDZT_ERR_TIMEOUT = 5
+EDZT_ERR_NUMERIC = 6
+ENGINE_FUSED = 0
+ENGINE_PLAIN = 1
+
+# Every symbol include/edzt.h declares.
+EXPORTS = (
+    "edzt_ctx_create", "edzt_ctx_destroy", "edzt_last_error", "edzt_version", "edzt_set_model",
+    "edzt_set_engine", "edzt_basis", "edzt_basis_rank", "edzt_sector_dim", "edzt_hx", "edzt_apply_c",
+    "edzt_lanczos_iteration", "edzt_diag_lanczos", "edzt_ground_state", "edzt_gs_dim",
+    "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
+    "edzt_kernel_stats", "edzt_reset_stats",
+)
+
+
+class EDError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"edzt error {code}: {msg}")
+        self.code = code
+
+
+def build(force: bool = False) -> str:
+    """Compile libedzt.so for sm_100a with nvcc (cross-compiles without a GPU)."""
+    args = ["make", "-s", "-C", PKG_DIR, "-j4"] + (["-B"] if force else []) + ["libedzt.so"]
+    subprocess.run(args, check=True)
+    return LIB_PATH
+
+
+_lib = None
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libedzt.so and declare argument types (no GPU needed to load)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise EDError(EDZT_ERR_STATE, f"{path} is missing: run build() (make -C {PKG_DIR})")
+    L = C.CDLL(path)
+    L.edzt_ctx_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+    L.edzt_ctx_destroy.argtypes = [_vp]
+    L.edzt_ctx_destroy.restype = None
+    L.edzt_last_error.argtypes = [_vp]
+    L.edzt_last_error.restype = C.c_char_p
+    L.edzt_version.restype = C.c_char_p
+    L.edzt_set_model.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp, _vp] + [C.c_double] * 5
+    L.edzt_set_engine.argtypes = [_vp, C.c_int]
+    L.edzt_basis.argtypes = [_vp, C.c_int, C.c_int, _ip, _ip, _vp, _vp]
+    L.edzt_basis_rank.argtypes = [_vp, C.c_int, _vp]
+    L.edzt_sector_dim.argtypes = [_vp, C.c_int, C.c_int]
+    L.edzt_sector_dim.restype = C.c_longlong
+    L.edzt_hx.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp, C.c_int]
+    L.edzt_apply_c.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_int, _vp]
+    L.edzt_lanczos_iteration.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
+    L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
+    L.edzt_ground_state.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_uint64, _ip, _dp, _vp, _vp]
+    L.edzt_gs_dim.argtypes = [_vp]
+    L.edzt_gs_dim.restype = C.c_longlong
+    L.edzt_green_diag.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.edzt_cluster_green_ftn.argtypes = [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]
+    L.edzt_solve.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_uint64, C.c_int, C.c_int, _vp, _ip, _dp, _vp, _vp]
+    L.edzt_launch_count.argtypes = [_vp]
+    L.edzt_launch_count.restype = C.c_longlong
+    L.edzt_get_stream.argtypes = [_vp, C.POINTER(C.c_void_p)]
+    L.edzt_kernel_stats.argtypes = [_vp, C.POINTER(C.c_longlong), _dp, _dp]
+    L.edzt_reset_stats.argtypes = [_vp]
+    _lib = L
+    return L
+
+
+def _ptr(a) -> int | None:
+    """Address of a numpy array or a torch tensor (device pointers pass through)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return int(a.data_ptr())
+    raise TypeError(f"unsupported buffer type {type(a)}")
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+class Model:
+    """Impurity model in the reference's shapes: em(norb,2), ek(nbath,2), vmk(norb,nbath,2)."""
+
+    def __init__(self, norb, nbath, em, ek, vmk, U, Up=None, Jex=0.0, Jp=None, mu=0.0):
+        self.norb, self.nbath = int(norb), int(nbath)
+        self.nsite = self.norb + self.nbath
+        self.em = np.asarray(em, dtype=np.float64).reshape(self.norb, 2)
+        self.ek = np.asarray(ek, dtype=np.float64).reshape(self.nbath, 2)
+        self.vmk = np.asarray(vmk, dtype=np.float64).reshape(self.norb, self.nbath, 2)
+        self.U = float(U)
+        self.Jex = float(Jex)
+        # rotational-invariance defaults of src/dmft_params.f90:90-96
+        self.Up = float(self.U - 2 * self.Jex) if (Up is None or Up < 0) else float(Up)
+        self.Jp = float(self.Jex) if (Jp is None or Jp < 0) else float(Jp)
+        self.mu = float(mu)
+
+    def fortran_arrays(self):
+        return (np.ascontiguousarray(self.em.ravel(order="F")),
+                np.ascontiguousarray(self.ek.ravel(order="F")),
+                np.ascontiguousarray(self.vmk.ravel(order="F")))
+
+
+def matsubara(nw: int, beta: float) -> np.ndarray:
+    """omega_n = (2n+1) pi / beta, n = 0..nw-1 (src/dmft_grid.f90:42-52 on one rank)."""
+    return (2.0 * np.arange(nw, dtype=np.float64) + 1.0) * np.pi / beta
+
+
+class Solver:
+    """One CUDA context of the ED solver (edzt_ctx)."""
+
+    def __init__(self, device: int = 0, engine: int = ENGINE_FUSED):
+        self._L = load_library()
+        h = C.c_void_p()
+        rc = self._L.edzt_ctx_create(int(device), C.byref(h))
+        if rc != EDZT_OK:
+            raise EDError(rc, "edzt_ctx_create failed (no CUDA device?)")
+        self._h = h
+        self.model: Model | None = None
+        self.set_engine(engine)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.edzt_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != EDZT_OK:
+            raise EDError(rc, self._L.edzt_last_error(self._h).decode())
+
+    def set_engine(self, engine: int):
+        self._check(self._L.edzt_set_engine(self._h, int(engine)))
+
+    def launch_count(self) -> int:
+        return int(self._L.edzt_launch_count(self._h))
+
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this context (all its kernels run there)."""
+        p = C.c_void_p()
+        self._check(self._L.edzt_get_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def kernel_stats(self) -> dict:
+        """Persistent Lanczos kernel: launches, device ms (CUDA events) and algorithmic bytes."""
+        n, ms, by = C.c_longlong(), C.c_double(), C.c_double()
+        self._check(self._L.edzt_kernel_stats(self._h, C.byref(n), C.byref(ms), C.byref(by)))
+        return dict(launches=n.value, ms=ms.value, bytes=by.value)
+
+    def reset_stats(self):
+        self._check(self._L.edzt_reset_stats(self._h))
+
+    def set_model(self, m: Model):
+        em, ek, vmk = m.fortran_arrays()
+        self._check(self._L.edzt_set_model(self._h, m.norb, m.nbath, _ptr(em), _ptr(ek), _ptr(vmk),
+                                           m.U, m.Up, m.Jex, m.Jp, m.mu))
+        self.model = m
+        self._keep = (em, ek, vmk)
+
+    def dim(self, ne_up: int, ne_dn: int) -> int:
+        return int(self._L.edzt_sector_dim(self._h, ne_up, ne_dn))
+
+    # generate_basis
+    def generate_basis(self, ne_up: int, ne_dn: int):
+        nup, ndn = C.c_int(), C.c_int()
+        self._check(self._L.edzt_basis(self._h, ne_up, ne_dn, C.byref(nup), C.byref(ndn), None, None))
+        up = np.zeros(max(nup.value, 1), dtype=np.uint32)
+        dn = np.zeros(max(ndn.value, 1), dtype=np.uint32)
+        self._check(self._L.edzt_basis(self._h, ne_up, ne_dn, None, None, _ptr(up), _ptr(dn)))
+        return up[: nup.value], dn[: ndn.value]
+
+    def basis_rank(self, ne: int) -> np.ndarray:
+        r = np.zeros(1 << self.model.nsite, dtype=np.int32)
+        self._check(self._L.edzt_basis_rank(self._h, ne, _ptr(r)))
+        return r
+
+    def hx(self, ne_up, ne_dn, x, y=None, py: bool = False):
+        """y = H x (py=False) or y += H x (py=True).  numpy in/out, or device tensors in place."""
+        if isinstance(x, np.ndarray) or not hasattr(x, "data_ptr"):
+            x = _f64(x)
+            out = np.array(y, dtype=np.float64, copy=True) if (py and y is not None) else np.zeros_like(x)
+            self._check(self._L.edzt_hx(self._h, ne_up, ne_dn, _ptr(x), _ptr(out), 1 if py else 0))
+            return out
+        self._check(self._L.edzt_hx(self._h, ne_up, ne_dn, _ptr(x), _ptr(y), 1 if py else 0))
+        return y
+
+    def apply_c(self, ne_up, ne_dn, vec, pm, iorb, ispin):
+        vec = _f64(vec)
+        d = 1 if pm == 1 else -1
+        ou = ne_up + (d if ispin == 1 else 0)
+        od = ne_dn + (d if ispin == 2 else 0)
+        out = np.zeros(max(self.dim(ou, od), 1))
+        self._check(self._L.edzt_apply_c(self._h, ne_up, ne_dn, _ptr(vec), pm, iorb, ispin, _ptr(out)))
+        return out[: self.dim(ou, od)]
+
+    def lanczos_iteration(self, ne_up, ne_dn, v_init, maxnstep):
+        v_init = _f64(v_init)
+        a = np.zeros(maxnstep)
+        b = np.zeros(maxnstep)
+        n = C.c_int()
+        self._check(self._L.edzt_lanczos_iteration(self._h, ne_up, ne_dn, _ptr(v_init), maxnstep, C.byref(n),
+                                                   _ptr(a), _ptr(b)))
+        return n.value, a, b
+
+    def diag_lanczos(self, ne_up, ne_dn, maxnstep, seed=0, stream=0):
+        ev, res = C.c_double(), C.c_double()
+        vec = np.zeros(self.dim(ne_up, ne_dn))
+        self._check(self._L.edzt_diag_lanczos(self._h, ne_up, ne_dn, maxnstep, C.c_uint64(seed),
+                                              C.c_uint64(stream), C.byref(ev), _ptr(vec), C.byref(res)))
+        return dict(e0=ev.value, vec=vec, residual=res.value)
+
+    def ground_state(self, sectors, maxnstep, seed=0, want_vec=True):
+        sec = np.ascontiguousarray(np.asarray(sectors, dtype=np.int32).reshape(-1, 2))
+        isec, e0 = C.c_int(), C.c_double()
+        es = np.zeros(len(sec))
+        vec = None
+        if want_vec:
+            vec = np.zeros(max(max(self.dim(int(u), int(d)) for u, d in sec), 1))
+        self._check(self._L.edzt_ground_state(self._h, len(sec), _ptr(sec), maxnstep, C.c_uint64(seed),
+                                              C.byref(isec), C.byref(e0), _ptr(vec), _ptr(es)))
+        out = dict(isector=isec.value, e0=e0.value, e_sector=es, sector=tuple(int(v) for v in sec[isec.value]))
+        if want_vec:
+            out["vec"] = vec[: int(self._L.edzt_gs_dim(self._h))].copy()
+        return out
+
+    def green_diag(self, iorb, ispin, maxnstep, omega):
+        omega = _f64(omega)
+        nw = omega.size
+        ap, bp, am, bm = (np.zeros(maxnstep) for _ in range(4))
+        g = np.zeros(2 * nw)
+        self._check(self._L.edzt_green_diag(self._h, iorb, ispin, maxnstep, nw, _ptr(omega), _ptr(ap), _ptr(bp),
+                                            _ptr(am), _ptr(bm), _ptr(g)))
+        return dict(g=g[0::2] + 1j * g[1::2], ap=ap, bp=bp, am=am, bm=bm)
+
+    def cluster_green_ftn(self, nspin, maxnstep, omega):
+        omega = _f64(omega)
+        nw = omega.size
+        norb = self.model.norb
+        G = np.zeros(2 * nw * norb * nspin)
+        coeffs = np.zeros(norb * 2 * 4 * maxnstep)
+        self._check(self._L.edzt_cluster_green_ftn(self._h, nspin, maxnstep, nw, _ptr(omega), _ptr(G),
+                                                   _ptr(coeffs)))
+        Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, norb, nw)
+        return dict(G_cl=Gc, coeffs=coeffs.reshape(norb, 2, 4, maxnstep))
+
+    def solve(self, sectors, maxnstep, omega, nspin=1, seed=0):
+        """ground_state + cluster_green_ftn in one call (src/dmft.f90:76-78)."""
+        sec = np.ascontiguousarray(np.asarray(sectors, dtype=np.int32).reshape(-1, 2))
+        omega = _f64(omega)
+        nw = omega.size
+        norb = self.model.norb
+        G = np.zeros(2 * nw * norb * nspin)
+        isec, e0 = C.c_int(), C.c_double()
+        self._check(self._L.edzt_solve(self._h, len(sec), _ptr(sec), maxnstep, C.c_uint64(seed), nspin, nw,
+                                       _ptr(omega), C.byref(isec), C.byref(e0), _ptr(G), None))
+        return dict(isector=isec.value, e0=e0.value, G_cl=(G[0::2] + 1j * G[1::2]).reshape(nspin, norb, nw))

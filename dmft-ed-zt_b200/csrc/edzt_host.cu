@@ -1,0 +1,1299 @@
+// edzt_host.cu — host runtime and C ABI of libedzt.
+//
+// The host side of the replaced Fortran entry points: per-context model and
+// table caches, a device buffer pool, the batched-job runner that drives the
+// persistent Lanczos kernel, the plain (one kernel per BLAS-1 step) engine
+// used as the reference-structured GPU comparator, the drivers that restate
+// ground_state / diag_lanczos / cluster_green_ftn / green_diag, and the
+// extern "C" functions declared in include/edzt.h.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+#include <atomic>
+#include <algorithm>
+#include <cuda_runtime.h>
+#include "../../include/edzt.h"
+#include "edzt_internal.h"
+#include "tridiag.h"
+
+namespace {
+
+std::atomic<long long> g_launches{0};
+
+struct EdztError {
+    int code;
+    std::string msg;
+};
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t _e = (call);                                                                   \
+        if (_e != cudaSuccess)                                                                     \
+            throw EdztError{_e == cudaErrorMemoryAllocation ? EDZT_ERR_OOM : EDZT_ERR_CUDA,         \
+                            std::string(#call) + ": " + cudaGetErrorString(_e)};                   \
+    } while (0)
+
+#define CKLAUNCH()                                                                                 \
+    do {                                                                                           \
+        cudaError_t _e = cudaGetLastError();                                                       \
+        if (_e != cudaSuccess) throw EdztError{EDZT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(_e)}; \
+    } while (0)
+
+void arg_check(bool ok, const char* what)
+{
+    if (!ok) throw EdztError{EDZT_ERR_ARG, what};
+}
+
+// ---------------------------------------------------------------------------
+// device memory pool (grow-only cache of cudaMalloc blocks, reused by size)
+// ---------------------------------------------------------------------------
+class Pool {
+  public:
+    ~Pool() { release_all(); }
+    void* get(size_t bytes)
+    {
+        bytes = (bytes + 255) & ~(size_t)255;
+        if (bytes == 0) bytes = 256;
+        auto it = free_.lower_bound(bytes);
+        if (it != free_.end() && it->first <= 2 * bytes) {
+            void* p = it->second;
+            used_[p] = it->first;
+            free_.erase(it);
+            return p;
+        }
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            trim();
+            e = cudaMalloc(&p, bytes);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                throw EdztError{EDZT_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed"};
+            }
+        }
+        used_[p] = bytes;
+        return p;
+    }
+    void put(void* p)
+    {
+        if (!p) return;
+        auto it = used_.find(p);
+        if (it == used_.end()) return;
+        free_.emplace(it->second, p);
+        used_.erase(it);
+    }
+    void trim()
+    {
+        for (auto& kv : free_) cudaFree(kv.second);
+        free_.clear();
+    }
+    void release_all()
+    {
+        trim();
+        for (auto& kv : used_) cudaFree(kv.first);
+        used_.clear();
+    }
+
+  private:
+    std::multimap<size_t, void*> free_;
+    std::map<void*, size_t> used_;
+};
+
+// RAII lease of a pool block
+template <class T>
+struct Lease {
+    Pool* pool = nullptr;
+    T* p = nullptr;
+    Lease() = default;
+    Lease(Pool& pl, size_t n) : pool(&pl), p(static_cast<T*>(pl.get(n * sizeof(T)))) {}
+    Lease(const Lease&) = delete;
+    Lease& operator=(const Lease&) = delete;
+    Lease(Lease&& o) noexcept : pool(o.pool), p(o.p) { o.p = nullptr; }
+    Lease& operator=(Lease&& o) noexcept
+    {
+        if (this != &o) { reset(); pool = o.pool; p = o.p; o.p = nullptr; }
+        return *this;
+    }
+    ~Lease() { reset(); }
+    void reset()
+    {
+        if (p && pool) pool->put(p);
+        p = nullptr;
+    }
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    DevBuf() = default;
+    explicit DevBuf(size_t bytes) { CK(cudaMalloc(&p, bytes > 0 ? bytes : 16)); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { if (p) cudaFree(p); }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+bool is_device_ptr(const void* p)
+{
+    if (!p) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// ---------------------------------------------------------------------------
+// tables
+// ---------------------------------------------------------------------------
+struct StrTable {
+    int n = 0, count = 0;
+    std::unique_ptr<DevBuf> str, rank;
+};
+
+struct OpsTable {
+    int hw = 0;
+    std::unique_ptr<DevBuf> e1, hcnt, hidx, hval, imp, sub;
+};
+
+struct JHost {
+    int cnt;
+    JTrans t[EDZT_MAX_JT];
+};
+
+}  // namespace
+
+struct edzt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int engine = EDZT_ENGINE_FUSED;
+    bool has_model = false;
+    DevModel model{};
+    int P = 1;
+    bool has_j = false;
+    std::map<int, std::unique_ptr<StrTable>> str_tables;
+    std::map<std::pair<int, int>, std::unique_ptr<OpsTable>> ops_tables;
+    std::unique_ptr<DevBuf> wint, jcnt, jt;
+    Pool pool;
+    // resident ground state
+    bool has_gs = false;
+    int gs_up = 0, gs_dn = 0, gs_isector = -1;
+    double gs_e0 = 0.0, gs_residual = 0.0;
+    Lease<double> gs_vec;
+    // persistent-kernel scratch
+    std::unique_ptr<DevBuf> sync_words, status;
+    int grid_cache_smem = -1, grid_cache = 0, block_cache = 256;
+    // persistent-kernel statistics
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    long long st_launches = 0;
+    double st_ms = 0.0, st_bytes = 0.0;
+    // small host-visible scratch for the plain engine
+    double* pinned = nullptr;
+    std::unique_ptr<DevBuf> scal;          // device scalars
+    std::unique_ptr<DevBuf> dot_part;      // dot partials
+    long long launches_at_create = 0;
+};
+
+namespace {
+
+int nsite_of(const edzt_ctx* c) { return c->model.nsite; }
+
+StrTable& str_table(edzt_ctx* c, int n)
+{
+    auto it = c->str_tables.find(n);
+    if (it != c->str_tables.end()) return *it->second;
+    auto t = std::make_unique<StrTable>();
+    const int ns = nsite_of(c);
+    t->n = n;
+    t->count = (int)edzt_binom(ns, n);
+    t->str = std::make_unique<DevBuf>(sizeof(uint32_t) * (size_t)std::max(t->count, 1));
+    t->rank = std::make_unique<DevBuf>(sizeof(int32_t) * ((size_t)1 << ns));
+    launch_build_strings(ns, n, t->str->as<uint32_t>(), t->rank->as<int32_t>(), c->stream);
+    g_launches += 2;
+    CKLAUNCH();
+    StrTable& ref = *t;
+    c->str_tables.emplace(n, std::move(t));
+    return ref;
+}
+
+OpsTable& ops_table(edzt_ctx* c, int n, int sigma)
+{
+    auto key = std::make_pair(n, sigma);
+    auto it = c->ops_tables.find(key);
+    if (it != c->ops_tables.end()) return *it->second;
+    StrTable& st = str_table(c, n);
+    auto t = std::make_unique<OpsTable>();
+    const int norb = c->model.norb, nbath = c->model.nbath;
+    int hw = 0;
+    for (int a = 0; a < norb; a++)
+        for (int l = 0; l < nbath; l++)
+            if (std::fabs(c->model.vmk[a][l][sigma]) >= 1.0e-16) hw++;
+    t->hw = std::max(hw, 1);
+    const size_t cnt = (size_t)std::max(st.count, 1);
+    t->e1 = std::make_unique<DevBuf>(sizeof(double) * cnt);
+    t->hcnt = std::make_unique<DevBuf>(cnt);
+    t->hidx = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * t->hw);
+    t->hval = std::make_unique<DevBuf>(sizeof(double) * cnt * t->hw);
+    t->imp = std::make_unique<DevBuf>(cnt);
+    if (c->has_j) t->sub = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * c->P);
+    launch_build_spin_ops(c->model, sigma, n, st.count, st.str->as<uint32_t>(), st.rank->as<int32_t>(), t->hw,
+                          t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hidx->as<int32_t>(),
+                          t->hval->as<double>(), t->imp->as<uint8_t>(),
+                          t->sub ? t->sub->as<int32_t>() : nullptr, c->stream);
+    g_launches += 1;
+    CKLAUNCH();
+    OpsTable& ref = *t;
+    c->ops_tables.emplace(key, std::move(t));
+    return ref;
+}
+
+bool sector_valid(const edzt_ctx* c, int nu, int nd)
+{
+    return nu >= 0 && nd >= 0 && nu <= c->model.nsite && nd <= c->model.nsite;
+}
+
+long long sector_dim(const edzt_ctx* c, int nu, int nd)
+{
+    if (!sector_valid(c, nu, nd)) return 0;
+    return (long long)edzt_binom(c->model.nsite, nu) * (long long)edzt_binom(c->model.nsite, nd);
+}
+
+DevSector make_sector(edzt_ctx* c, int nu, int nd)
+{
+    DevSector S{};
+    StrTable& su = str_table(c, nu);
+    StrTable& sd = str_table(c, nd);
+    OpsTable& ou = ops_table(c, nu, 0);
+    OpsTable& od = ops_table(c, nd, 1);
+    auto fill = [&](DevSpin& sp, StrTable& s, OpsTable& o) {
+        sp.count = s.count;
+        sp.hw = o.hw;
+        sp.str = s.str->as<uint32_t>();
+        sp.rank = s.rank->as<int32_t>();
+        sp.e1 = o.e1->as<double>();
+        sp.hcnt = o.hcnt->as<uint8_t>();
+        sp.hidx = o.hidx->as<int32_t>();
+        sp.hval = o.hval->as<double>();
+        sp.imp = o.imp->as<uint8_t>();
+        sp.sub = o.sub ? o.sub->as<int32_t>() : nullptr;
+    };
+    fill(S.up, su, ou);
+    fill(S.dn, sd, od);
+    S.dim = (long long)su.count * sd.count;
+    S.P = c->P;
+    S.has_j = c->has_j ? 1 : 0;
+    S.wint = c->wint->as<double>();
+    S.jcnt = c->jcnt->as<int>();
+    S.jt = c->jt->as<JTrans>();
+    return S;
+}
+
+// Interaction tables over impurity occupation patterns (pu, pd).
+// wint: impurity_hamiltonian.f90:119-141 without the em-mu terms (those are
+// one-body and live in e1).  Exchange transitions: :179-226.
+void build_model_tables(edzt_ctx* c)
+{
+    const DevModel& m = c->model;
+    const int norb = m.norb, P = 1 << norb;
+    c->P = P;
+    std::vector<double> w(P * P, 0.0);
+    std::vector<int> jc(P * P, 0);
+    std::vector<JTrans> jt((size_t)P * P * EDZT_MAX_JT);
+    bool any_j = false;
+    for (int pu = 0; pu < P; pu++)
+        for (int pd = 0; pd < P; pd++) {
+            double e = 0.0;
+            for (int a = 0; a < norb; a++) {
+                const int n1 = (pu >> a) & 1, n2 = (pd >> a) & 1;
+                e += m.U * n1 * n2;
+                for (int b = a + 1; b < norb; b++) {
+                    const int m1 = (pu >> b) & 1, m2 = (pd >> b) & 1;
+                    e += (m.Up - m.Jex) * (n1 * m1 + n2 * m2) + m.Up * (n1 * m2 + n2 * m1);
+                }
+            }
+            w[pu * P + pd] = e;
+            int cnt = 0;
+            if (m.Jp != 0.0) {
+                for (int i = 1; i <= norb; i++)
+                    for (int j = 1; j <= norb; j++) {
+                        if (i == j) continue;
+                        const int ni1 = (pu >> (i - 1)) & 1, ni2 = (pd >> (i - 1)) & 1;
+                        const int nj1 = (pu >> (j - 1)) & 1, nj2 = (pd >> (j - 1)) & 1;
+                        const int lo = std::min(i, j), hi = std::max(i, j);
+                        int par = 0;
+                        for (int k = lo; k <= hi - 1; k++) par += ((pu >> (k - 1)) & 1) + ((pd >> (k - 1)) & 1);
+                        const double s2 = (par & 1) ? -1.0 : 1.0;
+                        if (ni1 == 0 && nj1 != 0 && nj2 == 0 && ni2 != 0) {   // spin-flip :201-211
+                            JTrans t;
+                            t.pu2 = (pu & ~(1 << (j - 1))) | (1 << (i - 1));
+                            t.pd2 = (pd & ~(1 << (i - 1))) | (1 << (j - 1));
+                            t.c = -(s2 * m.Jp);
+                            jt[((size_t)pu * P + pd) * EDZT_MAX_JT + cnt++] = t;
+                        }
+                        if (ni1 == 0 && ni2 == 0 && nj1 != 0 && nj2 != 0) {   // pair-hop :215-225
+                            JTrans t;
+                            t.pu2 = (pu & ~(1 << (j - 1))) | (1 << (i - 1));
+                            t.pd2 = (pd & ~(1 << (j - 1))) | (1 << (i - 1));
+                            t.c = s2 * m.Jp;
+                            jt[((size_t)pu * P + pd) * EDZT_MAX_JT + cnt++] = t;
+                        }
+                    }
+            }
+            jc[pu * P + pd] = cnt;
+            any_j = any_j || cnt > 0;
+        }
+    c->has_j = any_j;
+    c->wint = std::make_unique<DevBuf>(sizeof(double) * P * P);
+    c->jcnt = std::make_unique<DevBuf>(sizeof(int) * P * P);
+    c->jt = std::make_unique<DevBuf>(sizeof(JTrans) * jt.size());
+    CK(cudaMemcpy(c->wint->p, w.data(), sizeof(double) * P * P, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->jcnt->p, jc.data(), sizeof(int) * P * P, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->jt->p, jt.data(), sizeof(JTrans) * jt.size(), cudaMemcpyHostToDevice));
+}
+
+// ---------------------------------------------------------------------------
+// host <-> device argument staging
+// ---------------------------------------------------------------------------
+struct InVec {
+    const double* d = nullptr;
+    Lease<double> tmp;
+    InVec(edzt_ctx* c, const double* p, long long n)
+    {
+        if (is_device_ptr(p)) { d = p; return; }
+        tmp = Lease<double>(c->pool, (size_t)std::max(n, 1LL));
+        if (n > 0) CK(cudaMemcpyAsync(tmp.p, p, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        d = tmp.p;
+    }
+};
+
+struct OutVec {
+    double* d = nullptr;
+    double* host = nullptr;
+    long long n = 0;
+    Lease<double> tmp;
+    edzt_ctx* c;
+    OutVec(edzt_ctx* cc, double* p, long long nn) : n(nn), c(cc)
+    {
+        if (is_device_ptr(p)) { d = p; return; }
+        host = p;
+        tmp = Lease<double>(c->pool, (size_t)std::max(n, 1LL));
+        d = tmp.p;
+    }
+    void preload()
+    {   // accumulate semantics need the caller's values on the device
+        if (host && n > 0) CK(cudaMemcpyAsync(d, host, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    }
+    void finish()
+    {
+        if (host && n > 0) {
+            CK(cudaMemcpyAsync(host, d, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+        }
+    }
+};
+
+void copy_out(edzt_ctx* c, void* dst, const void* src, size_t bytes)
+{
+    if (!dst || bytes == 0) return;
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream));
+}
+
+// ---------------------------------------------------------------------------
+// batched persistent Lanczos
+// ---------------------------------------------------------------------------
+struct JobSpec {
+    int nu = 0, nd = 0;
+    int mode = LZ_COEFF;
+    int init = LZ_INIT_HASH;
+    uint64_t key = 0;
+    ApplyCArgs ac{};
+    const double* ac_src = nullptr;
+    int maxnstep = 0;
+    const double* coeff = nullptr;   // device, EIGVEC
+    double* eig = nullptr;           // device, EIGVEC
+    double* a = nullptr;             // device [maxnstep]
+    double* b = nullptr;             // device [maxnstep]
+    // results
+    int nstep = 0;
+    double norm0 = 0.0;
+};
+
+int persistent_grid(edzt_ctx* c, size_t smem, int* block)
+{
+    if ((int)smem != c->grid_cache_smem) {
+        c->grid_cache = lz_grid_size(c->device, smem, &c->block_cache);
+        c->grid_cache_smem = (int)smem;
+    }
+    *block = c->block_cache;
+    return c->grid_cache;
+}
+
+void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
+{
+    const int nj = (int)specs.size();
+    if (nj == 0) return;
+    std::vector<LzJob> jobs(nj);
+    std::vector<Lease<double>> bufs;
+    bufs.reserve((size_t)nj * 4);
+    size_t smem = 0;
+    for (int j = 0; j < nj; j++) {
+        JobSpec& s = specs[j];
+        LzJob& J = jobs[j];
+        std::memset(&J, 0, sizeof(J));
+        J.S = make_sector(c, s.nu, s.nd);
+        const long long dim = J.S.dim;
+        for (int q = 0; q < 2; q++) {
+            bufs.emplace_back(c->pool, (size_t)dim);
+            J.Y[q] = bufs.back().p;
+            bufs.emplace_back(c->pool, (size_t)dim);
+            J.W[q] = bufs.back().p;
+        }
+        J.eig = s.eig;
+        J.coeff = s.coeff;
+        J.a = s.a;
+        J.b = s.b;
+        J.maxnstep = s.maxnstep;
+        J.mode = s.mode;
+        J.init = s.init;
+        J.key = s.key;
+        J.ac = s.ac;
+        J.ac_src = s.ac_src;
+        J.rows_per_tile = lz_rows_per_tile(J.S.up.count, J.S.dn.count);
+        J.ntiles = (J.S.dn.count + J.rows_per_tile - 1) / J.rows_per_tile;
+        smem = std::max(smem, lz_smem_bytes(J.S.up.count, J.rows_per_tile));
+        if (s.mode == LZ_COEFF) {
+            CK(cudaMemsetAsync(s.a, 0, sizeof(double) * s.maxnstep, c->stream));
+            CK(cudaMemsetAsync(s.b, 0, sizeof(double) * s.maxnstep, c->stream));
+        }
+    }
+    int block = 256;
+    const int G = persistent_grid(c, smem, &block);
+    if (G <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
+    std::vector<long long> prefix(nj + 1, 0);
+    long long slots = 0;
+    int max_steps = 0, max_eig = 0, n_coeff = 0;
+    for (int j = 0; j < nj; j++) {
+        LzJob& J = jobs[j];
+        J.tile0 = prefix[j];
+        prefix[j + 1] = prefix[j] + J.ntiles;
+        J.npart = std::min(G, J.ntiles);
+        J.slot0 = slots;
+        slots += J.npart;
+        max_steps = std::max(max_steps, J.maxnstep);
+        if (J.mode == LZ_EIGVEC) max_eig = std::max(max_eig, J.maxnstep);
+        else n_coeff++;
+    }
+    std::vector<LzState> st(nj);
+    for (int j = 0; j < nj; j++) {
+        std::memset(&st[j], 0, sizeof(LzState));
+        st[j].active = 1;
+    }
+    // device-side batch description (one block of the pool)
+    const size_t bytes_jobs = sizeof(LzJob) * nj, bytes_st = sizeof(LzState) * nj;
+    const size_t bytes_pre = sizeof(long long) * (nj + 1), bytes_part = sizeof(double) * 3 * (size_t)slots;
+    const size_t bytes_arr = sizeof(unsigned) * nj;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t total = al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part) + al(bytes_arr);
+    Lease<char> blob(c->pool, total);
+    char* base = blob.p;
+    LzJob* d_jobs = reinterpret_cast<LzJob*>(base);
+    LzState* d_st = reinterpret_cast<LzState*>(base + al(bytes_jobs));
+    long long* d_pre = reinterpret_cast<long long*>(base + al(bytes_jobs) + al(bytes_st));
+    double* d_part = reinterpret_cast<double*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre));
+    unsigned* d_arr = reinterpret_cast<unsigned*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part));
+    CK(cudaMemcpyAsync(d_jobs, jobs.data(), bytes_jobs, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_st, st.data(), bytes_st, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_pre, prefix.data(), bytes_pre, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(d_arr, 0, bytes_arr, c->stream));
+    unsigned sw[8] = {0, 0, (unsigned)n_coeff, 0, (unsigned)n_coeff, 0, 0, 0};
+    CK(cudaMemcpyAsync(c->sync_words->p, sw, sizeof(sw), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->status->p, 0, sizeof(int), c->stream));
+    LzBatch B;
+    B.njobs = nj;
+    B.grid = G;
+    B.block = block;
+    B.smem = smem;
+    B.total_tiles = prefix[nj];
+    B.max_steps = max_steps;
+    B.max_eig_steps = max_eig;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    CK(launch_lanczos_persistent(B, d_jobs, d_st, d_pre, d_part, d_arr, c->sync_words->as<unsigned>(),
+                                 c->status->as<int>(), c->stream));
+    CK(cudaEventRecord(c->ev1, c->stream));
+    g_launches += 1;
+    int status = 0;
+    CK(cudaMemcpyAsync(st.data(), d_st, bytes_st, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&status, c->status->p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (status == EDZT_DEV_BARRIER_TIMEOUT)
+        throw EdztError{EDZT_ERR_TIMEOUT, "persistent Lanczos kernel: grid barrier wait timed out"};
+    if (status != 0) throw EdztError{EDZT_ERR_CUDA, "persistent Lanczos kernel reported status " + std::to_string(status)};
+    double bytes = 0.0;
+    for (int j = 0; j < nj; j++) {
+        specs[j].nstep = (specs[j].mode == LZ_COEFF) ? st[j].nstep : specs[j].maxnstep;
+        specs[j].norm0 = st[j].norm0;
+        const double dim = (double)jobs[j].S.dim;
+        const double init = (specs[j].init == LZ_INIT_HASH) ? 8.0 : 16.0;
+        const double per_step = (specs[j].mode == LZ_COEFF) ? 24.0 : 40.0;
+        bytes += dim * (init + per_step * specs[j].nstep);
+    }
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->st_launches += 1;
+    c->st_ms += ms;
+    c->st_bytes += bytes;
+}
+
+// ---------------------------------------------------------------------------
+// plain engine: the reference's lanczos_iteration step by step, one kernel per
+// BLAS-1 operation and a host read of every reduction (src/lanczos_solver.f90)
+// ---------------------------------------------------------------------------
+double plain_dot(edzt_ctx* c, const double* x, const double* y, long long n)
+{
+    launch_dot(x, y, n, c->dot_part->as<double>(), c->scal->as<double>(), c->stream);
+    g_launches += 2;
+    CK(cudaMemcpyAsync(c->pinned, c->scal->p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return c->pinned[0];
+}
+
+// lanczos_iteration (lanczos_solver.f90:92-173); a, b host arrays [maxnstep].
+int plain_lanczos(edzt_ctx* c, const DevSector& S, const double* v_init, int maxnstep, double* a, double* b,
+                  double* norm_out, const double* coeff, double* eig)
+{
+    const long long n = S.dim;
+    Lease<double> v(c->pool, (size_t)n), w(c->pool, (size_t)n);
+    if (coeff == nullptr)
+        for (int i = 0; i < maxnstep; i++) { a[i] = 0.0; b[i] = 0.0; }
+    const double norm_v = std::sqrt(plain_dot(c, v_init, v_init, n));          // :128
+    if (norm_out) *norm_out = norm_v;
+    if (!(norm_v > 0.0)) return 0;
+    CK(cudaMemcpyAsync(w.p, v_init, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    launch_swap_scale(v.p, w.p, n, nullptr, norm_v, c->stream);                // w = v_init / norm_v :130
+    std::swap(v.p, w.p);
+    g_launches += 1;
+    if (eig) {                                                                 // :254-255
+        CK(cudaMemsetAsync(eig, 0, sizeof(double) * n, c->stream));
+        launch_axpy(eig, w.p, n, nullptr, coeff[0], 1.0, c->stream);
+        g_launches += 1;
+    }
+    launch_hx(S, w.p, v.p, 0, c->stream);                                      // :132
+    g_launches += 1;
+    CKLAUNCH();
+    int nstep;
+    if (!coeff) a[0] = plain_dot(c, w.p, v.p, n);                              // :134
+    if (maxnstep == 1) return 1;                                               // :137-141
+    launch_axpy(v.p, w.p, n, nullptr, a[0], -1.0, c->stream);                  // :143
+    g_launches += 1;
+    if (!coeff) b[1] = std::sqrt(plain_dot(c, v.p, v.p, n));                   // :144
+    int k = 2;
+    for (;;) {
+        if (b[k - 1] < 1.0e-16) { nstep = k - 1; if (!coeff) b[k - 1] = 0.0; break; }
+        launch_swap_scale(w.p, v.p, n, nullptr, b[k - 1], c->stream);          // :152-156
+        g_launches += 1;
+        if (eig) {                                                             // :279
+            launch_axpy(eig, w.p, n, nullptr, coeff[k - 1], 1.0, c->stream);
+            g_launches += 1;
+        }
+        launch_hx(S, w.p, v.p, 1, c->stream);                                  // :158
+        g_launches += 1;
+        if (!coeff) a[k - 1] = plain_dot(c, w.p, v.p, n);                      // :159
+        if (k >= maxnstep) { nstep = k; break; }                               // :161-164
+        launch_axpy(v.p, w.p, n, nullptr, a[k - 1], -1.0, c->stream);          // :166
+        g_launches += 1;
+        if (!coeff) b[k] = std::sqrt(plain_dot(c, v.p, v.p, n));               // :167
+        k = k + 1;
+    }
+    return nstep;
+}
+
+// ---------------------------------------------------------------------------
+// drivers
+// ---------------------------------------------------------------------------
+void require_model(edzt_ctx* c)
+{
+    if (!c->has_model) throw EdztError{EDZT_ERR_STATE, "no model: call edzt_set_model first"};
+}
+
+void check_sector(edzt_ctx* c, int nu, int nd)
+{
+    arg_check(sector_valid(c, nu, nd), "electron counts outside [0, nsite]");
+}
+
+// Normalise the eigenvector and compute |H g - E g|^2 (lanczos_solver.f90:291-297).
+double finish_eigvec(edzt_ctx* c, const DevSector& S, double* vec, double e0)
+{
+    const long long n = S.dim;
+    double* sc = c->scal->as<double>();
+    launch_dot(vec, vec, n, c->dot_part->as<double>(), sc, c->stream);
+    launch_scale_inv_sqrt(vec, n, sc, c->stream);                              // :291
+    Lease<double> v(c->pool, (size_t)n);
+    launch_hx(S, vec, v.p, 0, c->stream);
+    launch_axpy(v.p, vec, n, nullptr, e0, -1.0, c->stream);
+    g_launches += 6;
+    CKLAUNCH();
+    return plain_dot(c, v.p, v.p, n);
+}
+
+struct SectorResult {
+    int nstep = 0;
+    double e = HUGE_VAL;
+    std::vector<double> a, b, coeff;
+    bool ok = false;
+};
+
+// streams (nullable): start-vector stream of each sector; default stream i for sector i.
+void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnstep, uint64_t seed, int* isector,
+                       double* e0, double* gsvec, double* e_sector, const uint64_t* streams = nullptr)
+{
+    auto stream_of = [&](int i) { return streams ? streams[i] : (uint64_t)i; };
+    require_model(c);
+    arg_check(nsector >= 1 && sectors != nullptr, "nsector >= 1 and sectors required");
+    arg_check(maxnstep >= 1, "maxnstep >= 1");
+    for (int i = 0; i < nsector; i++) check_sector(c, sectors[2 * i], sectors[2 * i + 1]);
+    std::vector<SectorResult> res(nsector);
+    const int ns = nsite_of(c);
+    (void)ns;
+    c->has_gs = false;
+    if (c->engine == EDZT_ENGINE_FUSED) {
+        std::vector<JobSpec> specs;
+        std::vector<int> which;
+        Lease<double> ab(c->pool, (size_t)nsector * 2 * maxnstep);
+        for (int i = 0; i < nsector; i++) {
+            const int nu = sectors[2 * i], nd = sectors[2 * i + 1];
+            if (sector_dim(c, nu, nd) <= 0) continue;
+            JobSpec s;
+            s.nu = nu; s.nd = nd;
+            s.mode = LZ_COEFF;
+            s.init = LZ_INIT_HASH;
+            s.key = edzt_stream_key(seed, stream_of(i));
+            s.maxnstep = maxnstep;
+            s.a = ab.p + (size_t)(2 * i) * maxnstep;
+            s.b = ab.p + (size_t)(2 * i + 1) * maxnstep;
+            specs.push_back(s);
+            which.push_back(i);
+        }
+        run_jobs(c, specs);
+        std::vector<double> hab((size_t)nsector * 2 * maxnstep);
+        CK(cudaMemcpyAsync(hab.data(), ab.p, sizeof(double) * hab.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (size_t q = 0; q < specs.size(); q++) {
+            const int i = which[q];
+            SectorResult& r = res[i];
+            r.nstep = specs[q].nstep;
+            r.a.assign(hab.begin() + (size_t)(2 * i) * maxnstep, hab.begin() + (size_t)(2 * i + 1) * maxnstep);
+            r.b.assign(hab.begin() + (size_t)(2 * i + 1) * maxnstep, hab.begin() + (size_t)(2 * i + 2) * maxnstep);
+            if (r.nstep >= 1) {
+                r.coeff.resize(r.nstep);
+                r.ok = edzt::lowest_eigenpair(r.nstep, r.a.data(), r.b.data(), &r.e, r.coeff.data()) == 0;
+            }
+        }
+    }
+    // selection (ground_state.f90:62-68), strict with a 1e-10 relative tie band
+    int best = -1;
+    double beste = HUGE_VAL;
+    auto consider = [&](int i) {
+        const double tie = 1.0e-10 * std::max(1.0, std::fabs(beste));
+        if (best < 0 || res[i].e < beste - tie) { best = i; beste = res[i].e; }
+    };
+    if (c->engine == EDZT_ENGINE_FUSED) {
+        for (int i = 0; i < nsector; i++) {
+            if (e_sector) e_sector[i] = res[i].ok ? res[i].e : NAN;
+            if (res[i].ok) consider(i);
+        }
+        if (best < 0) throw EdztError{EDZT_ERR_NUMERIC, "no sector produced a ground state"};
+        const int nu = sectors[2 * best], nd = sectors[2 * best + 1];
+        const long long dim = sector_dim(c, nu, nd);
+        c->gs_vec = Lease<double>(c->pool, (size_t)dim);
+        SectorResult& r = res[best];
+        Lease<double> cf(c->pool, (size_t)r.nstep), ab(c->pool, (size_t)2 * maxnstep);
+        CK(cudaMemcpyAsync(cf.p, r.coeff.data(), sizeof(double) * r.nstep, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(ab.p, r.a.data(), sizeof(double) * maxnstep, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(ab.p + maxnstep, r.b.data(), sizeof(double) * maxnstep, cudaMemcpyHostToDevice, c->stream));
+        std::vector<JobSpec> ev(1);
+        ev[0].nu = nu; ev[0].nd = nd;
+        ev[0].mode = LZ_EIGVEC;
+        ev[0].init = LZ_INIT_HASH;
+        ev[0].key = edzt_stream_key(seed, stream_of(best));
+        ev[0].maxnstep = r.nstep;
+        ev[0].coeff = cf.p;
+        ev[0].eig = c->gs_vec.p;
+        ev[0].a = ab.p;
+        ev[0].b = ab.p + maxnstep;
+        run_jobs(c, ev);
+        DevSector S = make_sector(c, nu, nd);
+        c->gs_residual = finish_eigvec(c, S, c->gs_vec.p, r.e);
+        c->gs_up = nu; c->gs_dn = nd; c->gs_isector = best; c->gs_e0 = r.e;
+    } else {
+        // plain engine: diag_lanczos per sector, eigenvector for every sector
+        // as the reference does (ground_state.f90:30-73)
+        long long maxdim = 0;
+        for (int i = 0; i < nsector; i++) maxdim = std::max(maxdim, sector_dim(c, sectors[2 * i], sectors[2 * i + 1]));
+        Lease<double> vin(c->pool, (size_t)maxdim), vec(c->pool, (size_t)maxdim);
+        for (int i = 0; i < nsector; i++) {
+            const int nu = sectors[2 * i], nd = sectors[2 * i + 1];
+            if (e_sector) e_sector[i] = NAN;
+            if (sector_dim(c, nu, nd) <= 0) continue;
+            DevSector S = make_sector(c, nu, nd);
+            launch_fill_start(vin.p, S.dim, edzt_stream_key(seed, stream_of(i)), c->stream);   // :42-46
+            g_launches += 1;
+            SectorResult& r = res[i];
+            r.a.assign(maxnstep, 0.0);
+            r.b.assign(maxnstep, 0.0);
+            r.nstep = plain_lanczos(c, S, vin.p, maxnstep, r.a.data(), r.b.data(), nullptr, nullptr, nullptr);
+            if (r.nstep < 1) continue;
+            r.coeff.resize(r.nstep);
+            r.ok = edzt::lowest_eigenpair(r.nstep, r.a.data(), r.b.data(), &r.e, r.coeff.data()) == 0;
+            if (!r.ok) continue;
+            std::vector<double> bb = r.b;
+            plain_lanczos(c, S, vin.p, r.nstep, r.a.data(), bb.data(), nullptr, r.coeff.data(), vec.p);
+            const double resid = finish_eigvec(c, S, vec.p, r.e);
+            if (e_sector) e_sector[i] = r.e;
+            const int prev = best;
+            consider(i);
+            if (best != prev) {
+                c->gs_vec = Lease<double>(c->pool, (size_t)S.dim);
+                CK(cudaMemcpyAsync(c->gs_vec.p, vec.p, sizeof(double) * S.dim, cudaMemcpyDeviceToDevice, c->stream));
+                c->gs_up = nu; c->gs_dn = nd; c->gs_isector = i; c->gs_e0 = r.e; c->gs_residual = resid;
+            }
+        }
+        if (best < 0) throw EdztError{EDZT_ERR_NUMERIC, "no sector produced a ground state"};
+    }
+    c->has_gs = true;
+    *isector = c->gs_isector;
+    *e0 = c->gs_e0;
+    if (gsvec) copy_out(c, gsvec, c->gs_vec.p, sizeof(double) * sector_dim(c, c->gs_up, c->gs_dn));
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+// One c^+ or c run of green_diag.
+struct GreenRun {
+    int iorb, ispin, pm;
+    int nu, nd;            // excitation sector
+    int nstep = 0;
+    double norm0 = 0.0;
+    double* a = nullptr;   // device [maxnstep]
+    double* b = nullptr;
+};
+
+ApplyCArgs applyc_args(edzt_ctx* c, int in_up, int in_dn, int pm, int iorb, int ispin, int out_up, int out_dn)
+{
+    ApplyCArgs A{};
+    A.pm = pm; A.iorb = iorb; A.ispin = ispin;
+    A.nsite = nsite_of(c);
+    StrTable& ou = str_table(c, out_up);
+    StrTable& od = str_table(c, out_dn);
+    StrTable& iu = str_table(c, in_up);
+    StrTable& idn = str_table(c, in_dn);
+    A.out_nup = ou.count; A.out_ndn = od.count;
+    A.out_up_str = ou.str->as<uint32_t>();
+    A.out_dn_str = od.str->as<uint32_t>();
+    A.in_nup = iu.count;
+    A.in_up_rank = iu.rank->as<int32_t>();
+    A.in_dn_rank = idn.rank->as<int32_t>();
+    return A;
+}
+
+void excitation(int nu, int nd, int pm, int ispin, int* ou, int* od)
+{
+    const int d = (pm == 1) ? 1 : -1;
+    *ou = nu + (ispin == 1 ? d : 0);
+    *od = nd + (ispin == 2 ? d : 0);
+}
+
+// Runs all requested excitation Lanczos runs, then the continued fractions.
+// g_out[r]: complex [nw] per run (host), ab_out[r]: host a (maxnstep) + b.
+void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, const double* omega_dev,
+                std::vector<std::vector<double>>& g_out, std::vector<std::vector<double>>& ab_out)
+{
+    const int nr = (int)runs.size();
+    Lease<double> ab(c->pool, (size_t)std::max(nr, 1) * 2 * maxnstep);
+    CK(cudaMemsetAsync(ab.p, 0, sizeof(double) * (size_t)std::max(nr, 1) * 2 * maxnstep, c->stream));
+    for (int r = 0; r < nr; r++) {
+        runs[r].a = ab.p + (size_t)(2 * r) * maxnstep;
+        runs[r].b = ab.p + (size_t)(2 * r + 1) * maxnstep;
+    }
+    std::vector<int> live;
+    if (c->engine == EDZT_ENGINE_FUSED) {
+        std::vector<JobSpec> specs;
+        for (int r = 0; r < nr; r++) {
+            GreenRun& g = runs[r];
+            if (sector_dim(c, g.nu, g.nd) <= 0) continue;
+            JobSpec s;
+            s.nu = g.nu; s.nd = g.nd;
+            s.mode = LZ_COEFF;
+            s.init = LZ_INIT_APPLYC;
+            s.ac = applyc_args(c, c->gs_up, c->gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
+            s.ac_src = c->gs_vec.p;
+            s.maxnstep = maxnstep;
+            s.a = g.a; s.b = g.b;
+            specs.push_back(s);
+            live.push_back(r);
+        }
+        run_jobs(c, specs);
+        for (size_t q = 0; q < specs.size(); q++) {
+            runs[live[q]].nstep = specs[q].nstep;
+            runs[live[q]].norm0 = specs[q].norm0;
+        }
+    } else {
+        for (int r = 0; r < nr; r++) {
+            GreenRun& g = runs[r];
+            if (sector_dim(c, g.nu, g.nd) <= 0) continue;
+            DevSector S = make_sector(c, g.nu, g.nd);
+            Lease<double> vin(c->pool, (size_t)S.dim);
+            ApplyCArgs A = applyc_args(c, c->gs_up, c->gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
+            launch_apply_c(A, c->gs_vec.p, vin.p, c->stream);
+            g_launches += 1;
+            std::vector<double> ha(maxnstep), hb(maxnstep);
+            g.nstep = plain_lanczos(c, S, vin.p, maxnstep, ha.data(), hb.data(), &g.norm0, nullptr, nullptr);
+            CK(cudaMemcpyAsync(g.a, ha.data(), sizeof(double) * maxnstep, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemcpyAsync(g.b, hb.data(), sizeof(double) * maxnstep, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+        }
+    }
+    // b(1) = |c^(+)|gs>| (dmft_green.f90:219,249); continued fractions on the device
+    Lease<double> g(c->pool, (size_t)std::max(nr, 1) * 2 * nw);
+    CK(cudaMemsetAsync(g.p, 0, sizeof(double) * (size_t)std::max(nr, 1) * 2 * nw, c->stream));
+    std::vector<CFJob> cj;
+    for (int r = 0; r < nr; r++) {
+        GreenRun& gr = runs[r];
+        if (gr.nstep < 1) continue;
+        CK(cudaMemcpyAsync(gr.b, &gr.norm0, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CFJob J;
+        J.a = gr.a; J.b = gr.b;
+        // a breakdown after the first vector is evaluated with a zero second level
+        J.levels = (gr.nstep == 1 && maxnstep >= 2) ? 2 : gr.nstep;
+        J.zr_shift = (gr.pm == 1) ? c->gs_e0 : -c->gs_e0;
+        J.sign = (gr.pm == 1) ? -1.0 : 1.0;
+        J.g = g.p + (size_t)r * 2 * nw;
+        cj.push_back(J);
+    }
+    if (!cj.empty()) {
+        Lease<CFJob> dj(c->pool, cj.size());
+        CK(cudaMemcpyAsync(dj.p, cj.data(), sizeof(CFJob) * cj.size(), cudaMemcpyHostToDevice, c->stream));
+        launch_cf(dj.p, (int)cj.size(), omega_dev, nw, c->stream);
+        g_launches += 1;
+        CKLAUNCH();
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    std::vector<double> hg((size_t)std::max(nr, 1) * 2 * nw), hab((size_t)std::max(nr, 1) * 2 * maxnstep);
+    CK(cudaMemcpyAsync(hg.data(), g.p, sizeof(double) * hg.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hab.data(), ab.p, sizeof(double) * hab.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    g_out.assign(nr, {});
+    ab_out.assign(nr, {});
+    for (int r = 0; r < nr; r++) {
+        g_out[r].assign(hg.begin() + (size_t)r * 2 * nw, hg.begin() + (size_t)(r + 1) * 2 * nw);
+        ab_out[r].assign(hab.begin() + (size_t)(2 * r) * maxnstep, hab.begin() + (size_t)(2 * r + 2) * maxnstep);
+    }
+}
+
+void require_gs(edzt_ctx* c)
+{
+    if (!c->has_gs) throw EdztError{EDZT_ERR_STATE, "no resident ground state: call edzt_ground_state first"};
+}
+
+// cluster_green_ftn (dmft_green.f90:47-126)
+void cluster_green_impl(edzt_ctx* c, int nspin, int maxnstep, int nw, const double* omega, double* G_cl,
+                        double* coeffs)
+{
+    require_model(c);
+    require_gs(c);
+    arg_check(nspin == 1 || nspin == 2, "nspin must be 1 or 2");
+    arg_check(maxnstep >= 1 && nw >= 0, "maxnstep >= 1, nw >= 0");
+    const int norb = c->model.norb;
+    const bool even = !(nspin == 2 || c->gs_up != c->gs_dn);                    // :76-80
+    std::vector<GreenRun> runs;
+    for (int iorb = 1; iorb <= norb; iorb++)
+        for (int ispin = 1; ispin <= (even ? 1 : 2); ispin++)
+            for (int pm = 1; pm <= 2; pm++) {
+                GreenRun g;
+                g.iorb = iorb; g.ispin = ispin; g.pm = pm;
+                excitation(c->gs_up, c->gs_dn, pm, ispin, &g.nu, &g.nd);
+                runs.push_back(g);
+            }
+    InVec om(c, omega, nw);
+    std::vector<std::vector<double>> gs, abs_;
+    green_runs(c, runs, maxnstep, nw, om.d, gs, abs_);
+    std::vector<double> Gh((size_t)2 * nw * norb * nspin, 0.0);
+    std::vector<double> ch((size_t)norb * 2 * 4 * maxnstep, 0.0);
+    int r = 0;
+    for (int iorb = 1; iorb <= norb; iorb++) {
+        std::vector<double> g1(2 * nw, 0.0), g2(2 * nw, 0.0);
+        for (int ispin = 1; ispin <= (even ? 1 : 2); ispin++) {
+            std::vector<double>& gg = (ispin == 1) ? g1 : g2;
+            for (int pm = 1; pm <= 2; pm++, r++) {
+                for (int q = 0; q < 2 * nw; q++) gg[q] += gs[r][q];
+                const double* a = abs_[r].data();
+                const double* b = abs_[r].data() + maxnstep;
+                double* dst = ch.data() + ((size_t)(iorb - 1) * 2 + (ispin - 1)) * 4 * maxnstep;
+                double* da = dst + (pm == 1 ? 0 : 2) * maxnstep;
+                double* db = dst + (pm == 1 ? 1 : 3) * maxnstep;
+                std::memcpy(da, a, sizeof(double) * maxnstep);
+                std::memcpy(db, b, sizeof(double) * maxnstep);
+            }
+        }
+        if (even) {   // spin-down rows repeat spin-up (:102-109)
+            double* s1 = ch.data() + ((size_t)(iorb - 1) * 2) * 4 * maxnstep;
+            std::memcpy(s1 + 4 * maxnstep, s1, sizeof(double) * 4 * maxnstep);
+        }
+        for (int iw = 0; iw < nw; iw++) {                                       // :111-118
+            const size_t o1 = 2 * ((size_t)iw + (size_t)nw * (iorb - 1));
+            const size_t o2 = 2 * ((size_t)iw + (size_t)nw * ((iorb - 1) + (size_t)norb));
+            if (nspin == 1 && even) {
+                Gh[o1] = g1[2 * iw]; Gh[o1 + 1] = g1[2 * iw + 1];
+            } else if (nspin == 1) {
+                Gh[o1] = 0.5 * (g1[2 * iw] + g2[2 * iw]);
+                Gh[o1 + 1] = 0.5 * (g1[2 * iw + 1] + g2[2 * iw + 1]);
+            } else {
+                Gh[o1] = g1[2 * iw]; Gh[o1 + 1] = g1[2 * iw + 1];
+                Gh[o2] = g2[2 * iw]; Gh[o2 + 1] = g2[2 * iw + 1];
+            }
+        }
+    }
+    if (G_cl) copy_out(c, G_cl, Gh.data(), sizeof(double) * Gh.size());
+    if (coeffs) copy_out(c, coeffs, ch.data(), sizeof(double) * ch.size());
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+void green_diag_impl(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, const double* omega, double* ap,
+                     double* bp, double* am, double* bm, double* g)
+{
+    require_model(c);
+    require_gs(c);
+    arg_check(iorb >= 1 && iorb <= c->model.norb && (ispin == 1 || ispin == 2), "bad iorb/ispin");
+    arg_check(maxnstep >= 1 && nw >= 0, "maxnstep >= 1, nw >= 0");
+    std::vector<GreenRun> runs(2);
+    for (int pm = 1; pm <= 2; pm++) {
+        GreenRun& gr = runs[pm - 1];
+        gr.iorb = iorb; gr.ispin = ispin; gr.pm = pm;
+        excitation(c->gs_up, c->gs_dn, pm, ispin, &gr.nu, &gr.nd);
+    }
+    InVec om(c, omega, nw);
+    std::vector<std::vector<double>> gs, abs_;
+    green_runs(c, runs, maxnstep, nw, om.d, gs, abs_);
+    std::vector<double> gsum(2 * nw, 0.0);
+    for (int r = 0; r < 2; r++)
+        for (int q = 0; q < 2 * nw; q++) gsum[q] += gs[r][q];
+    copy_out(c, ap, abs_[0].data(), sizeof(double) * maxnstep);
+    copy_out(c, bp, abs_[0].data() + maxnstep, sizeof(double) * maxnstep);
+    copy_out(c, am, abs_[1].data(), sizeof(double) * maxnstep);
+    copy_out(c, bm, abs_[1].data() + maxnstep, sizeof(double) * maxnstep);
+    copy_out(c, g, gsum.data(), sizeof(double) * 2 * nw);
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+template <class F>
+int guarded(edzt_ctx* c, F&& f)
+{
+    if (!c) return EDZT_ERR_ARG;
+    try {
+        CK(cudaSetDevice(c->device));
+        f();
+        c->err.clear();
+        return EDZT_OK;
+    } catch (const EdztError& e) {
+        c->err = e.msg;
+        return e.code;
+    } catch (const std::exception& e) {
+        c->err = e.what();
+        return EDZT_ERR_CUDA;
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* edzt_version(void) { return "edzt-b200 0.1 (sm_100a)"; }
+
+int edzt_ctx_create(int device, edzt_ctx** out)
+{
+    if (!out) return EDZT_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return EDZT_ERR_CUDA;
+    }
+    edzt_ctx* c = new edzt_ctx();
+    c->device = device;
+    int rc = guarded(c, [&] {
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        edzt_init_binomials(device);
+        c->sync_words = std::make_unique<DevBuf>(64);
+        c->status = std::make_unique<DevBuf>(64);
+        c->scal = std::make_unique<DevBuf>(sizeof(double) * 32);
+        c->dot_part = std::make_unique<DevBuf>(sizeof(double) * dot_partials_size());
+        CK(cudaMallocHost((void**)&c->pinned, sizeof(double) * 32));
+        CK(cudaEventCreate(&c->ev0));
+        CK(cudaEventCreate(&c->ev1));
+        c->launches_at_create = g_launches.load();
+    });
+    if (rc != EDZT_OK) {
+        edzt_ctx_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return EDZT_OK;
+}
+
+void edzt_ctx_destroy(edzt_ctx* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->gs_vec.reset();
+    c->pool.release_all();
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* edzt_last_error(const edzt_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+long long edzt_launch_count(const edzt_ctx* c) { return c ? g_launches.load() - c->launches_at_create : 0; }
+
+int edzt_get_stream(edzt_ctx* c, void** stream)
+{
+    if (!c || !stream) return EDZT_ERR_ARG;
+    *stream = (void*)c->stream;
+    return EDZT_OK;
+}
+
+int edzt_kernel_stats(edzt_ctx* c, long long* launches, double* ms, double* bytes)
+{
+    if (!c) return EDZT_ERR_ARG;
+    if (launches) *launches = c->st_launches;
+    if (ms) *ms = c->st_ms;
+    if (bytes) *bytes = c->st_bytes;
+    return EDZT_OK;
+}
+
+int edzt_reset_stats(edzt_ctx* c)
+{
+    if (!c) return EDZT_ERR_ARG;
+    c->st_launches = 0;
+    c->st_ms = 0.0;
+    c->st_bytes = 0.0;
+    return EDZT_OK;
+}
+
+int edzt_set_engine(edzt_ctx* c, int engine)
+{
+    return guarded(c, [&] {
+        arg_check(engine == EDZT_ENGINE_FUSED || engine == EDZT_ENGINE_PLAIN, "unknown engine");
+        c->engine = engine;
+    });
+}
+
+int edzt_set_model(edzt_ctx* c, int norb, int nbath, const double* em, const double* ek, const double* vmk,
+                   double U, double Up, double Jex, double Jp, double mu)
+{
+    return guarded(c, [&] {
+        arg_check(norb >= 1 && norb <= EDZT_MAX_NORB, "norb must be in [1, 4]");
+        arg_check(nbath >= 0 && norb + nbath <= EDZT_MAX_NSITE, "norb + nbath must be <= 20");
+        arg_check(em != nullptr && (nbath == 0 || (ek != nullptr && vmk != nullptr)), "em/ek/vmk required");
+        DevModel m{};
+        m.norb = norb; m.nbath = nbath; m.nsite = norb + nbath;
+        for (int s = 0; s < 2; s++) {
+            for (int a = 0; a < norb; a++) m.em[a][s] = em[a + norb * s];
+            for (int l = 0; l < nbath; l++) m.ek[l][s] = ek[l + nbath * s];
+            for (int a = 0; a < norb; a++)
+                for (int l = 0; l < nbath; l++) m.vmk[a][l][s] = vmk[a + norb * (l + nbath * s)];
+        }
+        m.U = U; m.Up = Up; m.Jex = Jex; m.Jp = Jp; m.mu = mu;
+        const bool same_nsite = c->has_model && c->model.nsite == m.nsite;
+        if (!same_nsite) c->str_tables.clear();
+        c->ops_tables.clear();
+        c->model = m;
+        c->has_model = true;
+        c->has_gs = false;
+        build_model_tables(c);
+    });
+}
+
+long long edzt_sector_dim(edzt_ctx* c, int ne_up, int ne_dn)
+{
+    if (!c || !c->has_model) return 0;
+    return sector_dim(c, ne_up, ne_dn);
+}
+
+int edzt_basis(edzt_ctx* c, int ne_up, int ne_dn, int* nup, int* ndn, uint32_t* up, uint32_t* dn)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        check_sector(c, ne_up, ne_dn);
+        StrTable& su = str_table(c, ne_up);
+        StrTable& sd = str_table(c, ne_dn);
+        if (nup) *nup = su.count;
+        if (ndn) *ndn = sd.count;
+        if (up) copy_out(c, up, su.str->p, sizeof(uint32_t) * su.count);
+        if (dn) copy_out(c, dn, sd.str->p, sizeof(uint32_t) * sd.count);
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int edzt_basis_rank(edzt_ctx* c, int ne, int32_t* rank)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        arg_check(ne >= 0 && ne <= c->model.nsite && rank != nullptr, "bad electron count or null rank");
+        StrTable& s = str_table(c, ne);
+        copy_out(c, rank, s.rank->p, sizeof(int32_t) * ((size_t)1 << c->model.nsite));
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int edzt_hx(edzt_ctx* c, int ne_up, int ne_dn, const double* x, double* y, int accumulate)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        check_sector(c, ne_up, ne_dn);
+        arg_check(x != nullptr && y != nullptr, "x and y required");
+        DevSector S = make_sector(c, ne_up, ne_dn);
+        InVec xi(c, x, S.dim);
+        OutVec yo(c, y, S.dim);
+        if (accumulate) yo.preload();
+        launch_hx(S, xi.d, yo.d, accumulate ? 1 : 0, c->stream);
+        g_launches += 1;
+        CKLAUNCH();
+        yo.finish();
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int edzt_apply_c(edzt_ctx* c, int ne_up, int ne_dn, const double* vec, int pm, int iorb, int ispin, double* vec_out)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        check_sector(c, ne_up, ne_dn);
+        arg_check(pm == 1 || pm == 2, "pm must be 1 or 2");
+        arg_check(iorb >= 1 && iorb <= c->model.norb && (ispin == 1 || ispin == 2), "bad iorb/ispin");
+        arg_check(vec != nullptr && vec_out != nullptr, "vec and vec_out required");
+        int ou, od;
+        excitation(ne_up, ne_dn, pm, ispin, &ou, &od);
+        arg_check(sector_dim(c, ou, od) > 0, "output sector is empty");
+        ApplyCArgs A = applyc_args(c, ne_up, ne_dn, pm, iorb, ispin, ou, od);
+        InVec vi(c, vec, sector_dim(c, ne_up, ne_dn));
+        OutVec vo(c, vec_out, sector_dim(c, ou, od));
+        launch_apply_c(A, vi.d, vo.d, c->stream);
+        g_launches += 1;
+        CKLAUNCH();
+        vo.finish();
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int edzt_lanczos_iteration(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, int* nstep,
+                           double* a, double* b)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        check_sector(c, ne_up, ne_dn);
+        arg_check(v_init && nstep && a && b && maxnstep >= 1, "bad arguments");
+        const long long dim = sector_dim(c, ne_up, ne_dn);
+        arg_check(dim > 0, "empty sector");
+        InVec vi(c, v_init, dim);
+        std::vector<double> ha(maxnstep, 0.0), hb(maxnstep, 0.0);
+        if (c->engine == EDZT_ENGINE_FUSED) {
+            Lease<double> ab(c->pool, (size_t)2 * maxnstep);
+            std::vector<JobSpec> specs(1);
+            JobSpec& s = specs[0];
+            s.nu = ne_up; s.nd = ne_dn;
+            s.mode = LZ_COEFF;
+            s.init = LZ_INIT_COPY;
+            s.ac_src = vi.d;
+            s.maxnstep = maxnstep;
+            s.a = ab.p; s.b = ab.p + maxnstep;
+            run_jobs(c, specs);
+            CK(cudaMemcpyAsync(ha.data(), ab.p, sizeof(double) * maxnstep, cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaMemcpyAsync(hb.data(), ab.p + maxnstep, sizeof(double) * maxnstep, cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            *nstep = specs[0].nstep;
+        } else {
+            DevSector S = make_sector(c, ne_up, ne_dn);
+            *nstep = plain_lanczos(c, S, vi.d, maxnstep, ha.data(), hb.data(), nullptr, nullptr, nullptr);
+        }
+        copy_out(c, a, ha.data(), sizeof(double) * maxnstep);
+        copy_out(c, b, hb.data(), sizeof(double) * maxnstep);
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int edzt_diag_lanczos(edzt_ctx* c, int ne_up, int ne_dn, int maxnstep, uint64_t seed, uint64_t stream,
+                      double* eigval, double* eigvec, double* residual)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        check_sector(c, ne_up, ne_dn);
+        arg_check(eigval != nullptr && maxnstep >= 1, "bad arguments");
+        const long long dim = sector_dim(c, ne_up, ne_dn);
+        arg_check(dim > 0, "empty sector");
+        // a one-sector ground_state on the requested start-vector stream
+        std::vector<int> sec = {ne_up, ne_dn};
+        int is = 0;
+        double e0 = 0.0;
+        ground_state_impl(c, 1, sec.data(), maxnstep, seed, &is, &e0, nullptr, nullptr, &stream);
+        *eigval = e0;
+        if (eigvec) copy_out(c, eigvec, c->gs_vec.p, sizeof(double) * dim);
+        if (residual) *residual = c->gs_residual;
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int edzt_ground_state(edzt_ctx* c, int nsector, const int* sectors, int maxnstep, uint64_t seed, int* isector,
+                      double* e0, double* gsvec, double* e_sector)
+{
+    return guarded(c, [&] {
+        arg_check(isector != nullptr && e0 != nullptr, "isector and e0 required");
+        ground_state_impl(c, nsector, sectors, maxnstep, seed, isector, e0, gsvec, e_sector);
+    });
+}
+
+long long edzt_gs_dim(edzt_ctx* c)
+{
+    if (!c || !c->has_gs) return 0;
+    return sector_dim(c, c->gs_up, c->gs_dn);
+}
+
+int edzt_green_diag(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, const double* omega, double* ap,
+                    double* bp, double* am, double* bm, double* g)
+{
+    return guarded(c, [&] {
+        arg_check(ap && bp && am && bm && g && (omega || nw == 0), "bad arguments");
+        green_diag_impl(c, iorb, ispin, maxnstep, nw, omega, ap, bp, am, bm, g);
+    });
+}
+
+int edzt_cluster_green_ftn(edzt_ctx* c, int nspin, int maxnstep, int nw, const double* omega, double* G_cl,
+                           double* coeffs)
+{
+    return guarded(c, [&] {
+        arg_check(G_cl != nullptr && (omega || nw == 0), "bad arguments");
+        cluster_green_impl(c, nspin, maxnstep, nw, omega, G_cl, coeffs);
+    });
+}
+
+int edzt_solve(edzt_ctx* c, int nsector, const int* sectors, int maxnstep, uint64_t seed, int nspin, int nw,
+               const double* omega, int* isector, double* e0, double* G_cl, double* coeffs)
+{
+    return guarded(c, [&] {
+        arg_check(isector && e0 && G_cl && (omega || nw == 0), "bad arguments");
+        ground_state_impl(c, nsector, sectors, maxnstep, seed, isector, e0, nullptr, nullptr);
+        cluster_green_impl(c, nspin, maxnstep, nw, omega, G_cl, coeffs);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// edzt_internal.h — host-side declarations shared by the CUDA translation
+// units of libedzt (not part of the public C ABI; see include/edzt.h).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "edzt_device.cuh"
+
+// Impurity model as the kernels see it.  Shapes follow the reference's
+// Fortran arrays em(norb,2), ek(nbath,2), vmk(norb,nbath,2)
+// (src/impurity_hamiltonian.f90:80-84), stored here with the spin index last.
+struct DevModel {
+    int norb, nbath, nsite;
+    double em[EDZT_MAX_NORB][2];
+    double ek[EDZT_MAX_NSITE][2];
+    double vmk[EDZT_MAX_NORB][EDZT_MAX_NSITE][2];
+    double U, Up, Jex, Jp, mu;
+};
+
+// ---- tables.cu -------------------------------------------------------------
+void edzt_init_binomials(int device);
+uint64_t edzt_binom(int n, int k);
+// Fills str[C(nsite,n)] (ascending) and rank[2^nsite] on the device.
+void launch_build_strings(int nsite, int n, uint32_t* str, int32_t* rank, cudaStream_t s);
+// Per-string tables of one spin species (sigma = 0 up, 1 down) for a model.
+void launch_build_spin_ops(const DevModel& m, int sigma, int n, int count, const uint32_t* str,
+                           const int32_t* rank, int hw, double* e1, uint8_t* hcnt, int32_t* hidx,
+                           double* hval, uint8_t* imp, int32_t* sub, cudaStream_t s);
+
+// ---- kernels.cu: standalone (non-persistent) kernels ------------------------
+int hx_rows_per_tile(int nup, int ndn);
+void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s);
+// Deterministic dot product: result written to *out (device).  partials needs
+// dot_partials_size() doubles.
+int dot_partials_size();
+void launch_dot(const double* a, const double* b, long long n, double* partials, double* out, cudaStream_t s);
+// Scalars come from *p when p is non-null, else from the value argument.
+void launch_swap_scale(double* w, double* v, long long n, const double* bk_p, double bk, cudaStream_t s);
+void launch_axpy(double* y, const double* x, long long n, const double* alpha_p, double alpha, double sign,
+                 cudaStream_t s);
+void launch_scale_inv_sqrt(double* x, long long n, const double* nrm2, cudaStream_t s);
+void launch_fill_start(double* v, long long n, uint64_t key, cudaStream_t s);
+void launch_copy(double* dst, const double* src, long long n, cudaStream_t s);
+
+void launch_apply_c(const ApplyCArgs& A, const double* in, double* out, cudaStream_t s);
+
+// Continued fractions (src/numeric_utils.f90:11-44) for many runs at once.
+struct CFJob {
+    const double* a;      // [levels]
+    const double* b;      // [levels], b[0] = ||c^(+)|gs>||
+    int levels;           // number of CF levels (0: contributes nothing)
+    double zr_shift;      // real part of z: +E0 for c^+, -E0 for c
+    double sign;          // -1: z - a (continued_fraction_p), +1: z + a (continued_fraction_m)
+    double* g;            // [nw] complex interleaved, written (levels >= 1)
+};
+void launch_cf(const CFJob* jobs_dev, int njobs, const double* omega, int nw, cudaStream_t s);
+
+// ---- lanczos.cu: persistent fused Lanczos over a batch of jobs ------------
+enum LzMode { LZ_COEFF = 0, LZ_EIGVEC = 1 };
+enum LzInit { LZ_INIT_HASH = 0, LZ_INIT_APPLYC = 1, LZ_INIT_COPY = 2 };
+
+struct LzJob {
+    DevSector S;
+    double* Y[2];
+    double* W[2];
+    double* eig;          // EIGVEC: output eigenvector (unnormalised)
+    const double* coeff;  // EIGVEC: ground eigenvector of the tridiagonal [nstep]
+    double* a;            // [maxnstep]
+    double* b;            // [maxnstep]
+    int maxnstep;         // COEFF: LanczosSteps; EIGVEC: nstep of the coefficient pass
+    int mode;
+    int init;
+    int rows_per_tile;
+    int ntiles;
+    int npart;            // participating CTAs = min(grid, ntiles)
+    long long tile0;      // first tile of this job in the global tile list
+    long long slot0;      // first partial-sum slot
+    uint64_t key;         // LZ_INIT_HASH
+    ApplyCArgs ac;        // LZ_INIT_APPLYC
+    const double* ac_src; // LZ_INIT_APPLYC: source vector (the ground state); LZ_INIT_COPY: start vector
+};
+
+struct LzState {
+    int active;           // 1 while the run is going
+    int nstep;            // result: number of valid Lanczos steps
+    int k;                // last completed step
+    int need_exact;       // 1: b_{k+1} is being summed exactly in an extra phase
+    double a_prev;        // a_k, used to form w_{k+1}
+    double b_cur;         // b_{k+1}, the next normaliser
+    double norm0;         // ||v_init||
+    double spare;
+};
+
+struct LzBatch {
+    int njobs;
+    int grid;
+    int block;
+    size_t smem;
+    long long total_tiles;
+    int max_steps;
+    int max_eig_steps;
+};
+
+// Number of co-resident CTAs the persistent kernel gets for a given shared-memory size.
+int lz_grid_size(int device, size_t smem, int* block_out);
+// Runs the persistent kernel; jobs/state live on the device.  Returns a
+// cudaError_t; *dev_status receives the kernel's own status word.
+cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, LzState* state,
+                                      const long long* tile_prefix, double* partials,
+                                      unsigned* arrive, unsigned* sync_words, int* status,
+                                      cudaStream_t s);
+size_t lz_smem_bytes(int nup, int rows_per_tile);
+int lz_rows_per_tile(int nup, int ndn);

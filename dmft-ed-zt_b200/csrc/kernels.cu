@@ -1,0 +1,229 @@
+// kernels.cu — standalone (one launch per operation) sm_100a kernels:
+// H.v, the BLAS-1 steps of the plain Lanczos drop-in, apply_c and the
+// continued fractions.  The fused persistent Lanczos lives in lanczos.cu.
+#include <cuda_runtime.h>
+#include "edzt_internal.h"
+#include "hv_row.cuh"
+
+static constexpr int kHxThreads = 256;
+static constexpr int kHxTargetElems = 2048;
+
+int hx_rows_per_tile(int nup, int ndn)
+{
+    int r = kHxTargetElems / (nup > 0 ? nup : 1);
+    if (r < 1) r = 1;
+    if (r > ndn) r = ndn;
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// H.v: y = H x (accumulate = 0) or y = y + H x (accumulate = 1), the `py`
+// flag of src/impurity_hamiltonian.f90:241-245.  One CTA per block of R full
+// rows; the rows are staged in shared memory for the up-spin hops.
+// ---------------------------------------------------------------------------
+template <bool ACC>
+__global__ void __launch_bounds__(kHxThreads) k_hx(DevSector S, const double* __restrict__ x,
+                                                   double* __restrict__ y, int R)
+{
+    extern __shared__ double xs[];
+    const int nup = S.up.count, ndn = S.dn.count;
+    const int r0 = blockIdx.x * R;
+    const int rows = min(R, ndn - r0);
+    const int n = rows * nup;
+    const long long g0 = (long long)r0 * nup;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) xs[e] = __ldg(x + g0 + e);
+    __syncthreads();
+    auto gather = [&](long long idx) { return __ldg(x + idx); };
+    int r = threadIdx.x / nup, iu = threadIdx.x - r * nup;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const int id = r0 + r;
+        double v = hv_row_element(S, iu, id, xs + r * nup, xs[e], gather);
+        if (ACC) v = y[g0 + e] + v;
+        y[g0 + e] = v;
+        iu += blockDim.x;
+        while (iu >= nup) { iu -= nup; ++r; }
+    }
+}
+
+void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s)
+{
+    const int nup = S.up.count, ndn = S.dn.count;
+    if (nup <= 0 || ndn <= 0) return;
+    const int R = hx_rows_per_tile(nup, ndn);
+    const int tiles = (ndn + R - 1) / R;
+    const size_t smem = (size_t)R * nup * sizeof(double);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_hx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_hx<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_set = true;
+    }
+    if (accumulate) k_hx<true><<<tiles, kHxThreads, smem, s>>>(S, x, y, R);
+    else k_hx<false><<<tiles, kHxThreads, smem, s>>>(S, x, y, R);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic dot product (mpi_dot_product, src/numeric_utils.f90:159-170):
+// fixed grid of partial sums, then one block sums the partials in order.
+// ---------------------------------------------------------------------------
+static constexpr int kDotBlocks = 592;
+static constexpr int kDotThreads = 256;
+
+int dot_partials_size() { return kDotBlocks; }
+
+__global__ void __launch_bounds__(kDotThreads) k_dot_partial(const double* __restrict__ a,
+                                                             const double* __restrict__ b, long long n,
+                                                             double* __restrict__ partials)
+{
+    __shared__ double scratch[32];
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        v[0] = fma(a[i], b[i], v[0]);
+    block_sum<1>(v, scratch);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
+__global__ void __launch_bounds__(kDotThreads) k_dot_final(const double* __restrict__ partials, int np,
+                                                           double* __restrict__ out)
+{
+    __shared__ double scratch[32];
+    double v[1] = {0.0};
+    for (int i = threadIdx.x; i < np; i += blockDim.x) v[0] += partials[i];
+    block_sum<1>(v, scratch);
+    if (threadIdx.x == 0) *out = v[0];
+}
+
+void launch_dot(const double* a, const double* b, long long n, double* partials, double* out, cudaStream_t s)
+{
+    k_dot_partial<<<kDotBlocks, kDotThreads, 0, s>>>(a, b, n, partials);
+    k_dot_final<<<1, kDotThreads, 0, s>>>(partials, kDotBlocks, out);
+}
+
+// w = v / b_k ; v = -b_k * w_old  (src/lanczos_solver.f90:152-156); *bk holds b_k.
+__global__ void k_swap_scale(double* __restrict__ w, double* __restrict__ v, long long n,
+                             const double* __restrict__ bk_p, double bk)
+{
+    const double b = bk_p ? *bk_p : bk;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double t = w[i];
+        w[i] = v[i] / b;
+        v[i] = -b * t;
+    }
+}
+
+void launch_swap_scale(double* w, double* v, long long n, const double* bk_p, double bk, cudaStream_t s)
+{
+    k_swap_scale<<<592, 256, 0, s>>>(w, v, n, bk_p, bk);
+}
+
+// y = y + (sign * alpha) * x  (daxpy with a device scalar)
+__global__ void k_axpy(double* __restrict__ y, const double* __restrict__ x, long long n,
+                       const double* __restrict__ alpha_p, double alpha, double sign)
+{
+    const double al = sign * (alpha_p ? *alpha_p : alpha);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        y[i] = fma(al, x[i], y[i]);
+}
+
+void launch_axpy(double* y, const double* x, long long n, const double* alpha_p, double alpha, double sign,
+                 cudaStream_t s)
+{
+    k_axpy<<<592, 256, 0, s>>>(y, x, n, alpha_p, alpha, sign);
+}
+
+// x = x / sqrt(*nrm2)
+__global__ void k_scale_inv_sqrt(double* __restrict__ x, long long n, const double* __restrict__ nrm2)
+{
+    const double nrm = sqrt(*nrm2);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        x[i] = x[i] / nrm;
+}
+
+void launch_scale_inv_sqrt(double* x, long long n, const double* nrm2, cudaStream_t s)
+{
+    k_scale_inv_sqrt<<<592, 256, 0, s>>>(x, n, nrm2);
+}
+
+__global__ void k_fill_start(double* __restrict__ v, long long n, uint64_t key)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        v[i] = edzt_u01(key, (uint64_t)i);
+}
+
+void launch_fill_start(double* v, long long n, uint64_t key, cudaStream_t s)
+{
+    k_fill_start<<<592, 256, 0, s>>>(v, n, key);
+}
+
+void launch_copy(double* dst, const double* src, long long n, cudaStream_t s)
+{
+    cudaMemcpyAsync(dst, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+}
+
+// ---------------------------------------------------------------------------
+// apply_c (src/ed_operator.f90:13-57), row-wise over the output sector.
+// ---------------------------------------------------------------------------
+__global__ void k_apply_c(ApplyCArgs A, const double* __restrict__ in, double* __restrict__ out)
+{
+    const long long n = (long long)A.out_nup * A.out_ndn;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = apply_c_value(A, in, i);
+}
+
+void launch_apply_c(const ApplyCArgs& A, const double* in, double* out, cudaStream_t s)
+{
+    const long long n = (long long)A.out_nup * A.out_ndn;
+    if (n <= 0) return;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_apply_c<<<(int)blocks, 256, 0, s>>>(A, in, out);
+}
+
+// ---------------------------------------------------------------------------
+// Continued fractions (src/numeric_utils.f90:11-44): one thread per (run, w).
+//   f = b_n^2/(z -/+ a_n);  f = b_i^2/(z -/+ a_i - f), i = n-1..1
+// Complex division by Smith's method.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cdiv_real(double num, double br, double bi, double* cr, double* ci)
+{
+    if (fabs(br) >= fabs(bi)) {
+        const double r = bi / br, den = br + bi * r;
+        *cr = num / den;
+        *ci = (-num * r) / den;
+    } else {
+        const double r = br / bi, den = bi + br * r;
+        *cr = (num * r) / den;
+        *ci = (-num) / den;
+    }
+}
+
+__global__ void k_cf(const CFJob* __restrict__ jobs, int njobs, const double* __restrict__ omega, int nw)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= njobs * nw) return;
+    const int jb = t / nw, iw = t - jb * nw;
+    const CFJob J = jobs[jb];
+    const int n = J.levels;
+    if (n < 1) return;
+    const double zr = J.zr_shift, zi = omega[iw];
+    double xr, xi;
+    cdiv_real(J.b[n - 1] * J.b[n - 1], zr + J.sign * J.a[n - 1], zi, &xr, &xi);
+    for (int i = n - 1; i >= 2; i--)
+        cdiv_real(J.b[i - 1] * J.b[i - 1], zr + J.sign * J.a[i - 1] - xr, zi - xi, &xr, &xi);
+    cdiv_real(J.b[0] * J.b[0], zr + J.sign * J.a[0] - xr, zi - xi, &xr, &xi);
+    J.g[2 * iw] = xr;
+    J.g[2 * iw + 1] = xi;
+}
+
+void launch_cf(const CFJob* jobs_dev, int njobs, const double* omega, int nw, cudaStream_t s)
+{
+    const int n = njobs * nw;
+    if (n <= 0) return;
+    k_cf<<<(n + 127) / 128, 128, 0, s>>>(jobs_dev, njobs, omega, nw);
+}

@@ -1,0 +1,160 @@
+/*
+ * edzt.h — C ABI of the B200 (sm_100a) zero-temperature ED impurity solver.
+ *
+ * Drop-in boundary for the hot path of yw-choi/DMFT-ED-ZT.  Each entry point
+ * replaces one Fortran procedure of the reference (cited per function); a
+ * Fortran host binds them through iso_c_binding (INTEGRATION.md gives the
+ * interface module).  The DMFT loop, lattice, grid and bath fit stay on the
+ * host unchanged.
+ *
+ * Conventions
+ *  - Every function returns EDZT_OK (0) or an error code; edzt_last_error()
+ *    gives the message.  The reference aborts through die()/stop instead; a
+ *    Fortran shim calls die() on a non-zero status.
+ *  - Arrays are FP64, laid out as the reference's Fortran arrays:
+ *      em(norb,2)        em[iorb + norb*ispin]
+ *      ek(nbath,2)       ek[jbath + nbath*ispin]
+ *      vmk(norb,nbath,2) vmk[iorb + norb*(jbath + nbath*ispin)]
+ *    (0-based here).  A sector vector of (ne_up, ne_dn) has
+ *    C(nsite,ne_up)*C(nsite,ne_dn) entries, index idn*nup + iup
+ *    (src/ed_basis.f90:132-135).  Complex arrays are interleaved (re, im).
+ *  - Vector arguments may be host or device pointers (CUDA unified
+ *    addressing tells them apart); host buffers are staged through the device.
+ *  - One host thread per context.  A context owns one GPU, one stream and the
+ *    device-resident state between calls (the ground state vector stays on
+ *    the device for the Green's-function runs).
+ *  - Electron counts, orbital and spin indices follow the reference
+ *    (iorb, ispin are 1-based; pm = 1 creates, pm = 2 annihilates).
+ */
+#ifndef EDZT_H
+#define EDZT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDZT_OK 0
+#define EDZT_ERR_ARG 1      /* invalid argument (sector, index, size)            */
+#define EDZT_ERR_CUDA 2     /* CUDA runtime error                                */
+#define EDZT_ERR_OOM 3      /* device allocation failed                          */
+#define EDZT_ERR_STATE 4    /* call out of order (no model / no ground state)    */
+#define EDZT_ERR_TIMEOUT 5  /* a bounded device-side wait ran out                */
+#define EDZT_ERR_NUMERIC 6  /* non-finite result / tridiagonal solve failed      */
+
+/* Lanczos engine selector (edzt_set_engine). */
+#define EDZT_ENGINE_FUSED 0 /* persistent batched kernel (default)               */
+#define EDZT_ENGINE_PLAIN 1 /* one kernel per BLAS-1 step, host-driven: the plain */
+                            /* one-solve-at-a-time GPU Lanczos of the reference  */
+
+typedef struct edzt_ctx edzt_ctx;
+
+/* Context on CUDA device `device`.  Replaces mpi_setup (src/mpi.f90:16-30):
+ * the GPU path has no MPI decomposition. */
+int edzt_ctx_create(int device, edzt_ctx **out);
+void edzt_ctx_destroy(edzt_ctx *ctx);
+const char *edzt_last_error(const edzt_ctx *ctx);
+/* Library version string. */
+const char *edzt_version(void);
+
+/* Impurity model: the dmft_params globals (src/dmft_params.f90:7-50) plus the
+ * (em, ek, vmk) arguments every reference routine carries.  Up and Jp are the
+ * final values (the reference defaults Up = U - 2J, Jp = J when the input is
+ * negative, src/dmft_params.f90:90-96; the caller applies that rule).
+ * nsite = norb + nbath <= 20, norb <= 4. */
+int edzt_set_model(edzt_ctx *ctx, int norb, int nbath, const double *em, const double *ek,
+                   const double *vmk, double U, double Up, double Jex, double Jp, double mu);
+
+/* Selects the Lanczos engine (EDZT_ENGINE_*). */
+int edzt_set_engine(edzt_ctx *ctx, int engine);
+
+/* generate_basis (src/ed_basis.f90:42-114): the ascending up and down bit
+ * strings of sector (ne_up, ne_dn).  nup/ndn receive C(nsite, ne_up/dn);
+ * up/dn (nullable, host or device) receive the strings.  Bit-exact hook. */
+int edzt_basis(edzt_ctx *ctx, int ne_up, int ne_dn, int *nup, int *ndn, uint32_t *up, uint32_t *dn);
+
+/* Rank table of one spin species (idx_up/idx_down of basis_t,
+ * src/ed_basis.f90:32-33,106-109), 0-based, -1 for strings outside the
+ * sector: rank[0 .. 2^nsite). */
+int edzt_basis_rank(edzt_ctx *ctx, int ne, int32_t *rank);
+
+/* Dimension C(nsite,ne_up)*C(nsite,ne_dn) of a sector (0 if empty). */
+long long edzt_sector_dim(edzt_ctx *ctx, int ne_up, int ne_dn);
+
+/* hx (src/impurity_hamiltonian.f90:77-247): y = H x, or y = y + H x when
+ * accumulate != 0 (the `py` flag).  x, y: sector vectors. */
+int edzt_hx(edzt_ctx *ctx, int ne_up, int ne_dn, const double *x, double *y, int accumulate);
+
+/* apply_c (src/ed_operator.f90:13-57): vec_out = c^+_{iorb,ispin} vec (pm=1)
+ * or c_{iorb,ispin} vec (pm=2).  vec is in sector (ne_up, ne_dn); vec_out in
+ * the N+-1 sector chosen as green_diag does (src/dmft_green.f90:204-210,
+ * 232-238).  Returns EDZT_ERR_ARG if that sector is empty. */
+int edzt_apply_c(edzt_ctx *ctx, int ne_up, int ne_dn, const double *vec, int pm, int iorb, int ispin,
+                 double *vec_out);
+
+/* lanczos_iteration (src/lanczos_solver.f90:92-173): three-term Lanczos from
+ * v_init without re-orthogonalisation.  a, b: [maxnstep] (host or device),
+ * zeroed then filled; b[0] = 0.  *nstep = steps taken.  Breakdown
+ * (b(k) < 1e-16) is tested before dividing and stops with nstep = k-1. */
+int edzt_lanczos_iteration(edzt_ctx *ctx, int ne_up, int ne_dn, const double *v_init, int maxnstep,
+                           int *nstep, double *a, double *b);
+
+/* diag_lanczos (src/lanczos_solver.f90:20-90) with a reproducible start
+ * vector (U[0,1) from (seed, stream)): lowest eigenvalue of the sector, its
+ * eigenvector (nullable) and the residual |H g - E g|^2 (nullable). */
+int edzt_diag_lanczos(edzt_ctx *ctx, int ne_up, int ne_dn, int maxnstep, uint64_t seed, uint64_t stream,
+                      double *eigval, double *eigvec, double *residual);
+
+/* ground_state (src/ground_state.f90:1-81): scans sectors[nsector][2] =
+ * (ne_up, ne_dn), keeps the lowest energy (a later sector wins only if lower
+ * by more than 1e-10*max(1,|E|)), and keeps its normalised vector resident
+ * on the device for edzt_cluster_green_ftn.  Sector i starts Lanczos from
+ * stream i of `seed`.  gsvec (nullable, host or device) receives the vector
+ * (gs%vec, src/eigpair.f90:5-9); e_sector (nullable) [nsector] the per-sector
+ * lowest energies. */
+int edzt_ground_state(edzt_ctx *ctx, int nsector, const int *sectors, int maxnstep, uint64_t seed,
+                      int *isector, double *e0, double *gsvec, double *e_sector);
+
+/* Dimension of the resident ground-state vector (0 if none). */
+long long edzt_gs_dim(edzt_ctx *ctx);
+
+/* green_diag (src/dmft_green.f90:177-260) on the resident ground state:
+ * c^+ and c Lanczos runs of maxnstep steps in the N+-1 sectors,
+ * b(1) = |c^(+)|gs>|, and g(iw) = CF_p(E0 + i w) + CF_m(-E0 + i w)
+ * (src/numeric_utils.f90:11-44).  ap, bp, am, bm: [maxnstep]; g: complex [nw]. */
+int edzt_green_diag(edzt_ctx *ctx, int iorb, int ispin, int maxnstep, int nw, const double *omega,
+                    double *ap, double *bp, double *am, double *bm, double *g);
+
+/* cluster_green_ftn (src/dmft_green.f90:47-126) on the resident ground
+ * state: G_cl(nw, norb, nspin) complex (column-major, interleaved) and,
+ * nullable, coeffs[norb][2][4][maxnstep] = (ap, bp, am, bm) per (orbital,
+ * spin): the rows the reference writes to g_coeffs.dat.  All c/c^+ runs of
+ * all orbitals and spins go to the device in one batched launch. */
+int edzt_cluster_green_ftn(edzt_ctx *ctx, int nspin, int maxnstep, int nw, const double *omega,
+                           double *G_cl, double *coeffs);
+
+/* One impurity solve: edzt_ground_state followed by edzt_cluster_green_ftn
+ * (the calls at src/dmft.f90:76-78).  gsvec, e_sector, coeffs nullable. */
+int edzt_solve(edzt_ctx *ctx, int nsector, const int *sectors, int maxnstep, uint64_t seed, int nspin,
+               int nw, const double *omega, int *isector, double *e0, double *G_cl, double *coeffs);
+
+/* Kernel launches issued by this context since creation (instrumentation). */
+long long edzt_launch_count(const edzt_ctx *ctx);
+
+/* The cudaStream_t every kernel of this context runs on (for event timing). */
+int edzt_get_stream(edzt_ctx *ctx, void **stream);
+
+/* Persistent Lanczos kernel statistics since the last reset: launches, total
+ * device time (CUDA events around each launch, ms) and algorithmic HBM bytes
+ * (24 B per state per coefficient step, 40 B per state per eigenvector step,
+ * 8 B per state for a generated start vector, 16 B per state for a copied or
+ * c/c^+-projected one). */
+int edzt_kernel_stats(edzt_ctx *ctx, long long *launches, double *ms, double *bytes);
+int edzt_reset_stats(edzt_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDZT_H */

@@ -1,0 +1,279 @@
+"""ctypes front end of the CPU oracle (oracle/edzt_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU legs as the checker; the product never imports it.
+Parity status: unpinned against the reference (no runnable reference, no
+reference tests); see the header of edzt_oracle.c for what pins it instead.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+_lib = None
+_lock = threading.Lock()
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with gcc (seconds)."""
+    src = os.path.join(HERE, "edzt_oracle.c")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE, "-B", "liboracle.so"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            build()
+            L = C.CDLL(LIB_PATH)
+            L.or_create.restype = C.c_void_p
+            L.or_create.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp] + [C.c_double] * 5
+            L.or_destroy.argtypes = [C.c_void_p]
+            L.or_sector_dim.restype = C.c_longlong
+            L.or_sector_dim.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            L.or_basis.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip]
+            L.or_generate_spin_basis.argtypes = [C.c_int, C.c_int, _ip, _ip]
+            L.or_icom.argtypes = [C.c_int, C.c_int]
+            L.or_hx.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, C.c_int]
+            L.or_hx_rows.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, C.c_longlong, C.c_longlong]
+            L.or_apply_c.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp]
+            L.or_lanczos_iteration.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _ip, _dp, _dp]
+            L.or_tridiag_lowest.argtypes = [C.c_int, _dp, _dp, _dp, _dp]
+            L.or_diag_lanczos.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64,
+                                          _dp, _dp, _dp, _ip, _dp, _dp]
+            L.or_ground_state.argtypes = [C.c_void_p, C.c_int, _ip, C.c_int, C.c_uint64, _ip, _dp, _dp,
+                                          _dp, _dp]
+            L.or_continued_fraction.argtypes = [C.c_double, C.c_double, C.c_int, _dp, _dp, C.c_int, _dp, _dp]
+            L.or_green_diag.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_double, C.c_int, C.c_int,
+                                        C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _ip]
+            L.or_cluster_green_ftn.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, C.c_double,
+                                               C.c_int, C.c_int, _dp, _dp, _dp]
+            L.or_start_vector.argtypes = [C.c_uint64, C.c_uint64, C.c_longlong, _dp]
+            L.or_dot.restype = C.c_double
+            L.or_dot.argtypes = [_dp, _dp, C.c_longlong]
+            L.or_num_threads.restype = C.c_int
+            L.or_set_num_threads.argtypes = [C.c_int]
+            _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def set_num_threads(n: int) -> None:
+    lib().or_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().or_num_threads())
+
+
+def spin_basis(nsite: int, n: int):
+    """Ascending popcount-n strings and the dense 1-based rank table (ed_basis.f90:76-113)."""
+    L = lib()
+    cnt = L.or_icom(nsite, n) if 0 <= n <= nsite else 0
+    strings = np.zeros(max(cnt, 1), dtype=np.int32)
+    idx = np.zeros(1 << nsite, dtype=np.int32)
+    got = L.or_generate_spin_basis(nsite, n, _i(strings), _i(idx))
+    return strings[:got].copy(), idx
+
+
+def start_vector(seed: int, stream: int, n: int) -> np.ndarray:
+    v = np.empty(max(n, 1), dtype=np.float64)
+    lib().or_start_vector(C.c_uint64(seed), C.c_uint64(stream), n, _d(v))
+    return v[:n]
+
+
+def dot(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return float(lib().or_dot(_d(a), _d(b), a.size))
+
+
+def tridiag_lowest(a: np.ndarray, b: np.ndarray, n: int):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    e0 = C.c_double()
+    z = np.zeros(max(n, 1), dtype=np.float64)
+    rc = lib().or_tridiag_lowest(n, _d(a), _d(b), C.byref(e0), _d(z))
+    if rc != 0:
+        raise ValueError("tridiag_lowest failed")
+    return e0.value, z[:n]
+
+
+def continued_fraction(z: complex, n: int, a, b, sign: int) -> complex:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    fr, fi = C.c_double(), C.c_double()
+    lib().or_continued_fraction(z.real, z.imag, n, _d(a), _d(b), sign, C.byref(fr), C.byref(fi))
+    return complex(fr.value, fi.value)
+
+
+def matsubara(nw: int, beta: float) -> np.ndarray:
+    """omega(i) = (2(i-1)+1) pi / beta, dmft_grid.f90:42-52 (one rank)."""
+    return np.array([(2.0 * float(i) + 1.0) * np.pi / beta for i in range(nw)], dtype=np.float64)
+
+
+class Oracle:
+    """One impurity model (em, ek, vmk, U, Up, J, Jp, mu) on the CPU.
+
+    em: (norb, 2); ek: (nbath, 2); vmk: (norb, nbath, 2) — the reference's
+    Fortran shapes; stored column-major as the reference lays them out.
+    """
+
+    def __init__(self, norb, nbath, em, ek, vmk, U, Up, Jex, Jp, mu):
+        self.norb, self.nbath = int(norb), int(nbath)
+        self.nsite = self.norb + self.nbath
+        self.em = np.asfortranarray(np.asarray(em, dtype=np.float64).reshape(self.norb, 2))
+        self.ek = np.asfortranarray(np.asarray(ek, dtype=np.float64).reshape(self.nbath, 2))
+        self.vmk = np.asfortranarray(np.asarray(vmk, dtype=np.float64).reshape(self.norb, self.nbath, 2))
+        self.U, self.Up, self.Jex, self.Jp, self.mu = map(float, (U, Up, Jex, Jp, mu))
+        emf = np.ascontiguousarray(self.em.ravel(order="F"))
+        ekf = np.ascontiguousarray(self.ek.ravel(order="F"))
+        vmf = np.ascontiguousarray(self.vmk.ravel(order="F"))
+        self._h = lib().or_create(self.norb, self.nbath, _d(emf), _d(ekf), _d(vmf),
+                                  self.U, self.Up, self.Jex, self.Jp, self.mu)
+        if not self._h:
+            raise ValueError("or_create rejected the model")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.or_destroy(h)
+            self._h = None
+
+    def model_dict(self) -> dict:
+        return dict(norb=self.norb, nbath=self.nbath, em=self.em.tolist(), ek=self.ek.tolist(),
+                    vmk=self.vmk.tolist(), U=self.U, Up=self.Up, Jex=self.Jex, Jp=self.Jp, mu=self.mu)
+
+    def dim(self, ne_up: int, ne_dn: int) -> int:
+        return int(lib().or_sector_dim(self._h, ne_up, ne_dn))
+
+    def basis(self, ne_up: int, ne_dn: int):
+        nup = lib().or_icom(self.nsite, ne_up)
+        ndn = lib().or_icom(self.nsite, ne_dn)
+        up = np.zeros(max(nup, 1), dtype=np.int32)
+        dn = np.zeros(max(ndn, 1), dtype=np.int32)
+        if lib().or_basis(self._h, ne_up, ne_dn, _i(up), _i(dn)) != 0:
+            raise ValueError("bad sector")
+        return up[:nup].copy(), dn[:ndn].copy()
+
+    def hx(self, ne_up: int, ne_dn: int, x: np.ndarray, y: np.ndarray | None = None, py: bool = False):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.array(y, dtype=np.float64, copy=True) if (py and y is not None) else np.zeros_like(x)
+        if lib().or_hx(self._h, ne_up, ne_dn, _d(x), _d(out), 1 if py else 0) != 0:
+            raise ValueError("bad sector")
+        return out
+
+    def hx_rows(self, ne_up: int, ne_dn: int, x: np.ndarray, r0: int, r1: int) -> np.ndarray:
+        """Rows [r0, r1) of H x (for spot checks of sectors too large for a full CPU H.v)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(x.size)
+        if lib().or_hx_rows(self._h, ne_up, ne_dn, _d(x), _d(y), r0, r1) != 0:
+            raise ValueError("bad sector")
+        return y[r0:r1].copy()
+
+    def apply_c(self, ne_up, ne_dn, vec, pm, iorb, ispin):
+        vec = np.ascontiguousarray(vec, dtype=np.float64)
+        d = 1 if pm == 1 else -1
+        oup = ne_up + (d if ispin == 1 else 0)
+        odn = ne_dn + (d if ispin == 2 else 0)
+        n = self.dim(oup, odn)
+        out = np.zeros(max(n, 1), dtype=np.float64)
+        rc = lib().or_apply_c(self._h, ne_up, ne_dn, _d(vec), pm, iorb, ispin, _d(out))
+        if rc < 0:
+            raise ValueError("bad apply_c arguments")
+        return out[:n]
+
+    def lanczos_iteration(self, ne_up, ne_dn, v_init, maxnstep):
+        v_init = np.ascontiguousarray(v_init, dtype=np.float64)
+        a = np.zeros(maxnstep)
+        b = np.zeros(maxnstep)
+        nstep = C.c_int()
+        if lib().or_lanczos_iteration(self._h, ne_up, ne_dn, _d(v_init), maxnstep, C.byref(nstep),
+                                      _d(a), _d(b)) != 0:
+            raise ValueError("bad sector")
+        return nstep.value, a, b
+
+    def diag_lanczos(self, ne_up, ne_dn, maxnstep, seed=0, stream=0, want_vec=True):
+        n = self.dim(ne_up, ne_dn)
+        ev = C.c_double()
+        res = C.c_double()
+        vec = np.zeros(n) if want_vec else None
+        nstep = C.c_int()
+        a = np.zeros(maxnstep)
+        b = np.zeros(maxnstep)
+        rc = lib().or_diag_lanczos(self._h, ne_up, ne_dn, maxnstep, C.c_uint64(seed), C.c_uint64(stream),
+                                   C.byref(ev), _d(vec), C.byref(res), C.byref(nstep), _d(a), _d(b))
+        if rc != 0:
+            raise ValueError("diag_lanczos failed")
+        return dict(e0=ev.value, vec=vec, residual=res.value, nstep=nstep.value, a=a, b=b)
+
+    def ground_state(self, sectors, maxnstep, seed=0):
+        sec = np.ascontiguousarray(np.asarray(sectors, dtype=np.int32).reshape(-1, 2))
+        maxdim = max(self.dim(int(u), int(d)) for u, d in sec)
+        vec = np.zeros(max(maxdim, 1))
+        es = np.zeros(len(sec))
+        isec = C.c_int()
+        e0 = C.c_double()
+        res = C.c_double()
+        rc = lib().or_ground_state(self._h, len(sec), _i(sec), maxnstep, C.c_uint64(seed), C.byref(isec),
+                                   C.byref(e0), _d(vec), _d(es), C.byref(res))
+        if rc != 0:
+            raise ValueError("ground_state failed")
+        u, d = sec[isec.value]
+        return dict(isector=isec.value, e0=e0.value, vec=vec[: self.dim(int(u), int(d))].copy(),
+                    e_sector=es, residual=res.value, sector=(int(u), int(d)))
+
+    def green_diag(self, ne_up, ne_dn, gsvec, e0, iorb, ispin, maxnstep, omega):
+        gsvec = np.ascontiguousarray(gsvec, dtype=np.float64)
+        omega = np.ascontiguousarray(omega, dtype=np.float64)
+        nw = omega.size
+        ap, bp, am, bm = (np.zeros(maxnstep) for _ in range(4))
+        g = np.zeros(2 * nw)
+        ns = np.zeros(2, dtype=np.int32)
+        rc = lib().or_green_diag(self._h, ne_up, ne_dn, _d(gsvec), e0, iorb, ispin, maxnstep, nw, _d(omega),
+                                 _d(ap), _d(bp), _d(am), _d(bm), _d(g), _i(ns))
+        if rc != 0:
+            raise ValueError("green_diag failed")
+        return dict(g=g[0::2] + 1j * g[1::2], ap=ap, bp=bp, am=am, bm=bm, nstep=(int(ns[0]), int(ns[1])))
+
+    def cluster_green_ftn(self, nspin, ne_up, ne_dn, gsvec, e0, maxnstep, omega):
+        gsvec = np.ascontiguousarray(gsvec, dtype=np.float64)
+        omega = np.ascontiguousarray(omega, dtype=np.float64)
+        nw = omega.size
+        G = np.zeros(2 * nw * self.norb * nspin)
+        coeffs = np.zeros(self.norb * 2 * 4 * maxnstep)
+        lib().or_cluster_green_ftn(self._h, nspin, ne_up, ne_dn, _d(gsvec), e0, maxnstep, nw, _d(omega),
+                                   _d(G), _d(coeffs))
+        Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, self.norb, nw)   # (ispin, iorb, iw)
+        return dict(G_cl=Gc, coeffs=coeffs.reshape(self.norb, 2, 4, maxnstep))
+
+    def dense_h(self, ne_up, ne_dn) -> np.ndarray:
+        """H assembled column by column from hx (the idea of debug.f90:13-57)."""
+        n = self.dim(ne_up, ne_dn)
+        H = np.zeros((n, n))
+        e = np.zeros(n)
+        for j in range(n):
+            e[:] = 0.0
+            e[j] = 1.0
+            H[:, j] = self.hx(ne_up, ne_dn, e)
+        return H

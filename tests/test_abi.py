@@ -1,0 +1,52 @@
+"""The C ABI library builds, loads without a GPU and exports every declared symbol."""
+
+import ctypes as C
+import os
+import re
+
+from conftest import ROOT
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "edzt.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(edzt_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_header_matches_python_mirror(pkg):
+    assert sorted(pkg.EXPORTS) == _declared()
+
+
+def test_library_exports_every_symbol(pkg):
+    pkg.build()
+    lib = C.CDLL(pkg.LIB_PATH)
+    for name in _declared():
+        assert hasattr(lib, name), name
+
+
+def test_version_and_null_context(pkg):
+    pkg.build()
+    L = pkg.load_library()
+    assert L.edzt_version().startswith(b"edzt-b200")
+    assert L.edzt_last_error(None) == b"null context"
+    assert L.edzt_hx(None, 1, 1, None, None, 0) == pkg.EDZT_ERR_ARG
+    assert L.edzt_launch_count(None) == 0
+
+
+def test_context_creation_fails_cleanly_without_gpu(pkg):
+    import torch
+    if torch.cuda.is_available():
+        return
+    pkg.build()
+    L = pkg.load_library()
+    h = C.c_void_p()
+    assert L.edzt_ctx_create(0, C.byref(h)) == pkg.EDZT_ERR_CUDA
+    assert not h.value
+
+
+def test_model_defaults(pkg):
+    import numpy as np
+    m = pkg.Model(2, 2, np.zeros((2, 2)), np.zeros((2, 2)), np.zeros((2, 2, 2)), U=2.0, Jex=0.5, mu=1.0)
+    assert m.Up == 1.0 and m.Jp == 0.5          # src/dmft_params.f90:90-96
+    w = pkg.matsubara(3, np.pi)
+    assert np.allclose(w, [1.0, 3.0, 5.0])

@@ -1,0 +1,149 @@
+"""GPU parity: kernel (c) Lanczos (fused persistent and plain engines), the
+ground-state scan and the Green's function, against the CPU oracle.
+
+Tolerances (the acceptance bar of the drop-in):
+  ground-state energy          |dE0| <= 1e-10 * max(1, |E0|)
+  first 50 Lanczos a_n, b_n    |d| <= 1e-8
+  G(i w_n)                     |dG| <= 1e-8
+Past the first ~50 steps an unreorthogonalised Lanczos amplifies rounding
+differences between any two FP64 implementations, so later coefficients are
+not compared element-wise.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import ab_compare_len, oracle_for, random_model
+
+pytestmark = pytest.mark.gpu
+E_TOL = 1e-10
+AB_TOL = 1e-8
+G_TOL = 1e-8
+
+
+def _e_ok(a, b):
+    return abs(a - b) <= E_TOL * max(1.0, abs(b))
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+def test_lanczos_iteration_coefficients(pkg, solver, oracle_mod, engine):
+    solver.set_engine(engine)
+    try:
+        rng = np.random.default_rng(77)
+        m = random_model(pkg, rng, 1, 9, spin_dep=True)
+        solver.set_model(m)
+        o = oracle_for(oracle_mod, m)
+        for nu, nd in [(5, 5), (4, 6), (1, 1), (0, 1)]:
+            v0 = oracle_mod.start_vector(11, 0, o.dim(nu, nd))
+            n_ref, a_ref, b_ref = o.lanczos_iteration(nu, nd, v0, 120)
+            n, a, b = solver.lanczos_iteration(nu, nd, v0, 120)
+            assert n == n_ref, (nu, nd)
+            k = ab_compare_len(b_ref, n)
+            assert np.abs(a[:k] - a_ref[:k]).max() <= AB_TOL
+            assert np.abs(b[:k] - b_ref[:k]).max() <= AB_TOL
+            assert b[0] == 0.0
+    finally:
+        solver.set_engine(0)
+
+
+def test_lanczos_breakdown_and_maxnstep_one(pkg, solver, oracle_mod):
+    rng = np.random.default_rng(5)
+    m = random_model(pkg, rng, 1, 3)
+    solver.set_model(m)
+    o = oracle_for(oracle_mod, m)
+    v0 = np.array([0.7])
+    for nu, nd in [(0, 0), (4, 4)]:                      # one-dimensional sectors
+        n, a, b = solver.lanczos_iteration(nu, nd, v0, 20)
+        n_ref, a_ref, b_ref = o.lanczos_iteration(nu, nd, v0, 20)
+        assert n == n_ref == 1
+        assert abs(a[0] - a_ref[0]) <= 1e-14 * max(1, abs(a_ref[0]))
+        assert np.all(b == 0.0)
+    v = oracle_mod.start_vector(1, 0, o.dim(2, 2))
+    n, a, b = solver.lanczos_iteration(2, 2, v, 1)         # maxnstep == 1 (:137-141)
+    n_ref, a_ref, _ = o.lanczos_iteration(2, 2, v, 1)
+    assert n == n_ref == 1 and abs(a[0] - a_ref[0]) < 1e-12
+
+
+def test_diag_lanczos(pkg, solver, oracle_mod):
+    rng = np.random.default_rng(41)
+    m = random_model(pkg, rng, 2, 6, J=0.5)
+    solver.set_model(m)
+    o = oracle_for(oracle_mod, m)
+    r = solver.diag_lanczos(4, 4, 150, seed=3, stream=2)
+    ref = o.diag_lanczos(4, 4, 150, seed=3, stream=2)
+    assert _e_ok(r["e0"], ref["e0"])
+    assert r["residual"] < 1e-10
+    assert abs(abs(r["vec"] @ ref["vec"]) - 1.0) < 1e-8
+
+
+@pytest.fixture(scope="module")
+def bethe(configs, oracle_mod):
+    cfg = configs.bethe_n6()
+    o = oracle_for(oracle_mod, cfg["model"])
+    gs = o.ground_state(cfg["sectors"], cfg["maxnstep"], seed=7)
+    omega = oracle_mod.matsubara(256, cfg["beta"])
+    nu, nd = gs["sector"]
+    cg = o.cluster_green_ftn(1, nu, nd, gs["vec"], gs["e0"], cfg["maxnstep"], omega)
+    return cfg, gs, omega, cg
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+def test_ground_state_and_green_bethe_n6(solver, bethe, engine):
+    cfg, gs_ref, omega, cg_ref = bethe
+    solver.set_engine(engine)
+    try:
+        solver.set_model(cfg["model"])
+        gs = solver.ground_state(cfg["sectors"], cfg["maxnstep"], seed=7)
+        assert gs["isector"] == gs_ref["isector"]
+        assert _e_ok(gs["e0"], gs_ref["e0"])
+        es, es_ref = gs["e_sector"], gs_ref["e_sector"]
+        for e, er in zip(es, es_ref):
+            assert _e_ok(e, er)
+        assert abs(abs(gs["vec"] @ gs_ref["vec"]) - 1.0) < 1e-8
+        cg = solver.cluster_green_ftn(1, cfg["maxnstep"], omega)
+        assert np.abs(cg["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
+        c, cr = cg["coeffs"], cg_ref["coeffs"]
+        for q in (0, 2):   # (a^+, b^+) and (a^-, b^-) of spin up
+            k = ab_compare_len(cr[0, 0, q + 1], cfg["maxnstep"])
+            assert np.abs(c[0, 0, q, :k] - cr[0, 0, q, :k]).max() <= AB_TOL
+            assert np.abs(c[0, 0, q + 1, :k] - cr[0, 0, q + 1, :k]).max() <= AB_TOL
+        bp1, bm1 = c[0, 0, 1, 0], c[0, 0, 3, 0]
+        assert abs(bp1 ** 2 + bm1 ** 2 - 1.0) < 1e-12           # {c, c^+} = 1
+    finally:
+        solver.set_engine(0)
+
+
+def test_kanamori_n10_solve(solver, configs, oracle_mod):
+    cfg = configs.kanamori_n10()
+    o = oracle_for(oracle_mod, cfg["model"])
+    gs_ref = o.ground_state(cfg["sectors"], cfg["maxnstep"], seed=1)
+    omega = oracle_mod.matsubara(128, cfg["beta"])
+    nu, nd = gs_ref["sector"]
+    cg_ref = o.cluster_green_ftn(2, nu, nd, gs_ref["vec"], gs_ref["e0"], cfg["maxnstep"], omega)
+    solver.set_model(cfg["model"])
+    gs = solver.ground_state(cfg["sectors"], cfg["maxnstep"], seed=1)
+    assert gs["isector"] == gs_ref["isector"] and _e_ok(gs["e0"], gs_ref["e0"])
+    cg = solver.cluster_green_ftn(2, cfg["maxnstep"], omega)
+    assert np.abs(cg["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
+
+
+def test_green_diag_matches_cluster(solver, bethe):
+    cfg, _, omega, cg_ref = bethe
+    solver.set_model(cfg["model"])
+    solver.ground_state(cfg["sectors"], cfg["maxnstep"], seed=7)
+    r = solver.green_diag(1, 1, cfg["maxnstep"], omega)
+    assert np.abs(r["g"] - cg_ref["G_cl"][0, 0]).max() <= G_TOL
+
+
+def test_solve_aim_n12(solver, configs, oracle_mod):
+    """The large single-solve workload (nsite 12, 9 sectors, 300 steps) end to end."""
+    cfg = configs.aim_n12()
+    o = oracle_for(oracle_mod, cfg["model"])
+    gs_ref = o.ground_state(cfg["sectors"], cfg["maxnstep"], seed=0)
+    omega = oracle_mod.matsubara(cfg["nw"], cfg["beta"])
+    nu, nd = gs_ref["sector"]
+    cg_ref = o.cluster_green_ftn(1, nu, nd, gs_ref["vec"], gs_ref["e0"], cfg["maxnstep"], omega)
+    solver.set_model(cfg["model"])
+    r = solver.solve(cfg["sectors"], cfg["maxnstep"], omega, nspin=1, seed=0)
+    assert r["isector"] == gs_ref["isector"] and _e_ok(r["e0"], gs_ref["e0"])
+    assert np.abs(r["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
