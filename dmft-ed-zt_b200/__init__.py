@@ -27,7 +27,9 @@ import subprocess
 import numpy as np
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG_DIR, "libedzt.so")
+# EDZT_LIBRARY selects another build of the same C ABI (e.g. one compiled with
+# device-side bounds checks); the default is the in-tree libedzt.so.
+LIB_PATH = os.environ.get("EDZT_LIBRARY") or os.path.join(PKG_DIR, "libedzt.so")
 REPO_ROOT = os.path.dirname(PKG_DIR)
 
 EDZT_OK = 0
@@ -58,6 +60,8 @@ class EDError(RuntimeError):
 
 def build(force: bool = False) -> str:
     """Compile libedzt.so for sm_100a with nvcc (cross-compiles without a GPU)."""
+    if os.environ.get("EDZT_LIBRARY"):
+        return LIB_PATH
     args = ["make", "-s", "-C", PKG_DIR, "-j4"] + (["-B"] if force else []) + ["libedzt.so"]
     subprocess.run(args, check=True)
     return LIB_PATH

@@ -15,6 +15,15 @@
 #define EDZT_MAX_P (1 << EDZT_MAX_NORB)
 #define EDZT_MAX_JT 12  // norb*(norb-1) spin-flip/pair-hop transitions per pattern pair
 
+// Packed hop word (kernel-side hopping tables): bits 0..19 the target
+// string's rank (C(20,10) < 2^20), bits 20..26 the index of the amplitude
+// V(a,l) in the spin's coefficient table, bit 31 the fermion sign.
+#define HOP_RANK_MASK 0xFFFFFu
+#define HOP_CIDX_SHIFT 20
+#define HOP_CIDX_MASK 0x7Fu
+#define HOP_SIGN 0x80000000u
+#define EDZT_MAX_COEF 128
+
 // One spin species of one sector: strings with a fixed electron count and
 // the per-string tables derived from the impurity model.
 struct DevSpin {
@@ -24,11 +33,19 @@ struct DevSpin {
     const int32_t* rank;    // [2^nsite] rank of a string, -1 if popcount != n
     const double* e1;       // [count] one-body energy: sum (em-mu) n_imp + sum ek n_bath
     const uint8_t* hcnt;    // [count] number of allowed impurity<->bath hops
-    const int32_t* hidx;    // [hw][count] target rank of each hop
-    const double* hval;     // [hw][count] signed amplitude of each hop
+    const uint32_t* hop;    // [hw][count] packed hop words
+    const double* coef;     // [ncoef] amplitudes V(a,l) of this spin, index a*nbath + l
+    int ncoef;
+    int pad;
     const uint8_t* imp;     // [count] impurity bits (sites 1..norb)
     const int32_t* sub;     // [count][P] rank after replacing the impurity bits (norb > 1)
 };
+
+__device__ __forceinline__ double hop_coef(uint32_t p, const double* coef)
+{
+    const double c = coef[(p >> HOP_CIDX_SHIFT) & HOP_CIDX_MASK];
+    return (p & HOP_SIGN) ? -c : c;
+}
 
 // Spin-flip / pair-hop transition between impurity patterns (pu, pd) -> (pu2, pd2).
 struct JTrans {
@@ -121,6 +138,24 @@ __device__ __forceinline__ int ld_acquire_s32(const int* p)
     return v;
 }
 
+// Optional device-side bounds checks (compiled in with -DEDZT_DEVICE_CHECKS):
+// the first failed check records (code, a, b, c) and the access is skipped.
+#ifdef EDZT_DEVICE_CHECKS
+static __device__ long long g_edzt_bad[4];
+static __device__ __noinline__ void edzt_record_bad(long long code, long long a, long long b, long long c)
+{
+    if (atomicCAS(reinterpret_cast<unsigned long long*>(&g_edzt_bad[0]), 0ull, (unsigned long long)code) == 0ull) {
+        g_edzt_bad[1] = a;
+        g_edzt_bad[2] = b;
+        g_edzt_bad[3] = c;
+    }
+}
+#define EDZT_OK_OR(cond, code, a, b, c, skip) \
+    if (!(cond)) { edzt_record_bad((code), (long long)(a), (long long)(b), (long long)(c)); skip; }
+#else
+#define EDZT_OK_OR(cond, code, a, b, c, skip)
+#endif
+
 // apply_c (src/ed_operator.f90:13-57) from sector `in` to sector `out`.
 struct ApplyCArgs {
     int pm, iorb, ispin;       // 1-based iorb/ispin as in the reference; pm 1 = c^+, 2 = c
@@ -150,10 +185,12 @@ __device__ __forceinline__ double apply_c_value(const ApplyCArgs& A, const doubl
         if ((A.pm == 1) != ((u & bit) != 0u)) return 0.0;
         par = __popc(u & (bit - 1u));
         j = (long long)id * A.in_nup + __ldg(A.in_up_rank + (u ^ bit));   // down rank unchanged
+        EDZT_OK_OR(__ldg(A.in_up_rank + (u ^ bit)) >= 0, 41, i, u, bit, return 0.0)
     } else {
         if ((A.pm == 1) != ((d & bit) != 0u)) return 0.0;
         par = __popc(u) + __popc(d & (bit - 1u));
         j = (long long)__ldg(A.in_dn_rank + (d ^ bit)) * A.in_nup + iu;   // up rank unchanged
+        EDZT_OK_OR(__ldg(A.in_dn_rank + (d ^ bit)) >= 0, 42, i, d, bit, return 0.0)
     }
     const double v = __ldg(in + j);
     return (par & 1) ? -v : v;

@@ -158,7 +158,7 @@ struct StrTable {
 
 struct OpsTable {
     int hw = 0;
-    std::unique_ptr<DevBuf> e1, hcnt, hidx, hval, imp, sub;
+    std::unique_ptr<DevBuf> e1, hcnt, hop, imp, sub;
 };
 
 struct JHost {
@@ -179,7 +179,7 @@ struct edzt_ctx {
     bool has_j = false;
     std::map<int, std::unique_ptr<StrTable>> str_tables;
     std::map<std::pair<int, int>, std::unique_ptr<OpsTable>> ops_tables;
-    std::unique_ptr<DevBuf> wint, jcnt, jt;
+    std::unique_ptr<DevBuf> wint, jcnt, jt, coef;
     Pool pool;
     // resident ground state
     bool has_gs = false;
@@ -238,14 +238,12 @@ OpsTable& ops_table(edzt_ctx* c, int n, int sigma)
     const size_t cnt = (size_t)std::max(st.count, 1);
     t->e1 = std::make_unique<DevBuf>(sizeof(double) * cnt);
     t->hcnt = std::make_unique<DevBuf>(cnt);
-    t->hidx = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * t->hw);
-    t->hval = std::make_unique<DevBuf>(sizeof(double) * cnt * t->hw);
+    t->hop = std::make_unique<DevBuf>(sizeof(uint32_t) * cnt * t->hw);
     t->imp = std::make_unique<DevBuf>(cnt);
     if (c->has_j) t->sub = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * c->P);
-    launch_build_spin_ops(c->model, sigma, n, st.count, st.str->as<uint32_t>(), st.rank->as<int32_t>(), t->hw,
-                          t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hidx->as<int32_t>(),
-                          t->hval->as<double>(), t->imp->as<uint8_t>(),
-                          t->sub ? t->sub->as<int32_t>() : nullptr, c->stream);
+    launch_build_spin_ops(c->model, sigma, st.count, st.str->as<uint32_t>(), st.rank->as<int32_t>(), t->hw,
+                          t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hop->as<uint32_t>(),
+                          t->imp->as<uint8_t>(), t->sub ? t->sub->as<int32_t>() : nullptr, c->stream);
     g_launches += 1;
     CKLAUNCH();
     OpsTable& ref = *t;
@@ -278,13 +276,15 @@ DevSector make_sector(edzt_ctx* c, int nu, int nd)
         sp.rank = s.rank->as<int32_t>();
         sp.e1 = o.e1->as<double>();
         sp.hcnt = o.hcnt->as<uint8_t>();
-        sp.hidx = o.hidx->as<int32_t>();
-        sp.hval = o.hval->as<double>();
+        sp.hop = o.hop->as<uint32_t>();
         sp.imp = o.imp->as<uint8_t>();
         sp.sub = o.sub ? o.sub->as<int32_t>() : nullptr;
     };
     fill(S.up, su, ou);
     fill(S.dn, sd, od);
+    S.up.coef = c->coef->as<double>();
+    S.dn.coef = c->coef->as<double>() + EDZT_MAX_COEF;
+    S.up.ncoef = S.dn.ncoef = c->model.norb * c->model.nbath;
     S.dim = (long long)su.count * sd.count;
     S.P = c->P;
     S.has_j = c->has_j ? 1 : 0;
@@ -349,6 +349,13 @@ void build_model_tables(edzt_ctx* c)
             any_j = any_j || cnt > 0;
         }
     c->has_j = any_j;
+    // hop amplitudes V(a,l) per spin, the coefficient tables the packed hop words index
+    std::vector<double> cf(2 * EDZT_MAX_COEF, 0.0);
+    for (int sg = 0; sg < 2; sg++)
+        for (int a = 0; a < norb; a++)
+            for (int l = 0; l < m.nbath; l++) cf[sg * EDZT_MAX_COEF + a * m.nbath + l] = m.vmk[a][l][sg];
+    c->coef = std::make_unique<DevBuf>(sizeof(double) * cf.size());
+    CK(cudaMemcpy(c->coef->p, cf.data(), sizeof(double) * cf.size(), cudaMemcpyHostToDevice));
     c->wint = std::make_unique<DevBuf>(sizeof(double) * P * P);
     c->jcnt = std::make_unique<DevBuf>(sizeof(int) * P * P);
     c->jt = std::make_unique<DevBuf>(sizeof(JTrans) * jt.size());
@@ -439,20 +446,27 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     const int nj = (int)specs.size();
     if (nj == 0) return;
     std::vector<LzJob> jobs(nj);
-    std::vector<Lease<double>> bufs;
-    bufs.reserve((size_t)nj * 4);
-    size_t smem = 0;
+    std::vector<Lease<double2>> bufs;
+    bufs.reserve((size_t)nj * 2);
+    int max_nup = 1, max_hw = 1;
     for (int j = 0; j < nj; j++) {
         JobSpec& s = specs[j];
         LzJob& J = jobs[j];
         std::memset(&J, 0, sizeof(J));
         J.S = make_sector(c, s.nu, s.nd);
+        max_nup = std::max(max_nup, J.S.up.count);
+        max_hw = std::max(max_hw, J.S.dn.hw);
+    }
+    // every job stages whole rows; the chunk height fills the same budget
+    const size_t budget = lz_smem_budget(max_nup, max_hw);
+    size_t smem = 0;
+    for (int j = 0; j < nj; j++) {
+        JobSpec& s = specs[j];
+        LzJob& J = jobs[j];
         const long long dim = J.S.dim;
         for (int q = 0; q < 2; q++) {
             bufs.emplace_back(c->pool, (size_t)dim);
-            J.Y[q] = bufs.back().p;
-            bufs.emplace_back(c->pool, (size_t)dim);
-            J.W[q] = bufs.back().p;
+            J.YW[q] = bufs.back().p;
         }
         J.eig = s.eig;
         J.coeff = s.coeff;
@@ -463,10 +477,9 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
         J.init = s.init;
         J.key = s.key;
         J.ac = s.ac;
-        J.ac_src = s.ac_src;
-        J.rows_per_tile = lz_rows_per_tile(J.S.up.count, J.S.dn.count);
-        J.ntiles = (J.S.dn.count + J.rows_per_tile - 1) / J.rows_per_tile;
-        smem = std::max(smem, lz_smem_bytes(J.S.up.count, J.rows_per_tile));
+        J.src = s.ac_src;
+        J.rmax = lz_rows_per_chunk(J.S.up.count, J.S.dn.count, J.S.dn.hw, budget);
+        smem = std::max(smem, lz_smem_bytes(J.S.up.count, J.S.dn.hw, J.rmax));
         if (s.mode == LZ_COEFF) {
             CK(cudaMemsetAsync(s.a, 0, sizeof(double) * s.maxnstep, c->stream));
             CK(cudaMemsetAsync(s.b, 0, sizeof(double) * s.maxnstep, c->stream));
@@ -475,16 +488,30 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     int block = 256;
     const int G = persistent_grid(c, smem, &block);
     if (G <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
+    // element partition: CTA b owns [lo(b), lo(b+1)) of the concatenated jobs
     std::vector<long long> prefix(nj + 1, 0);
+    for (int j = 0; j < nj; j++) prefix[j + 1] = prefix[j] + jobs[j].S.dim;
+    const long long E = prefix[nj];
+    for (int j = 0; j < nj; j++) { jobs[j].first_cta = -1; jobs[j].npart = 0; jobs[j].nspan = 0; }
+    {
+        int j = 0;
+        for (int b = 0; b < G; b++) {
+            const long long lo = lz_cta_lo(E, G, b), hi = lz_cta_lo(E, G, b + 1);
+            if (lo >= hi) continue;
+            while (j < nj && prefix[j + 1] <= lo) j++;
+            for (int q = j; q < nj && prefix[q] < hi; q++) {
+                if (jobs[q].first_cta < 0) jobs[q].first_cta = b;
+                jobs[q].npart++;
+                jobs[q].nspan = b - jobs[q].first_cta + 1;
+            }
+        }
+    }
     long long slots = 0;
     int max_steps = 0, max_eig = 0, n_coeff = 0;
     for (int j = 0; j < nj; j++) {
         LzJob& J = jobs[j];
-        J.tile0 = prefix[j];
-        prefix[j + 1] = prefix[j] + J.ntiles;
-        J.npart = std::min(G, J.ntiles);
         J.slot0 = slots;
-        slots += J.npart;
+        slots += J.nspan;
         max_steps = std::max(max_steps, J.maxnstep);
         if (J.mode == LZ_EIGVEC) max_eig = std::max(max_eig, J.maxnstep);
         else n_coeff++;
@@ -519,7 +546,8 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     B.grid = G;
     B.block = block;
     B.smem = smem;
-    B.total_tiles = prefix[nj];
+    B.total_elems = E;
+    B.pad = 0;
     B.max_steps = max_steps;
     B.max_eig_steps = max_eig;
     CK(cudaEventRecord(c->ev0, c->stream));
@@ -1080,6 +1108,22 @@ int edzt_kernel_stats(edzt_ctx* c, long long* launches, double* ms, double* byte
     if (bytes) *bytes = c->st_bytes;
     return EDZT_OK;
 }
+
+#ifdef EDZT_DEVICE_CHECKS
+// Checked builds only: the first failed device bounds check (code, a, b, c).
+int edzt_debug_bad(long long* out4)
+{
+    // first recorded violation of the three kernel modules, in that order
+    long long t[4] = {0, 0, 0, 0};
+    int (*fns[3])(long long*) = {lz_debug_bad, kernels_debug_bad, tables_debug_bad};
+    for (int q = 0; q < 3; q++) {
+        fns[q](t);
+        if (t[0] != 0) break;
+    }
+    for (int q = 0; q < 4; q++) out4[q] = t[q];
+    return 0;
+}
+#endif
 
 int edzt_reset_stats(edzt_ctx* c)
 {

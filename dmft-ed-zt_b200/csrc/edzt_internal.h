@@ -22,12 +22,12 @@ uint64_t edzt_binom(int n, int k);
 // Fills str[C(nsite,n)] (ascending) and rank[2^nsite] on the device.
 void launch_build_strings(int nsite, int n, uint32_t* str, int32_t* rank, cudaStream_t s);
 // Per-string tables of one spin species (sigma = 0 up, 1 down) for a model.
-void launch_build_spin_ops(const DevModel& m, int sigma, int n, int count, const uint32_t* str,
-                           const int32_t* rank, int hw, double* e1, uint8_t* hcnt, int32_t* hidx,
-                           double* hval, uint8_t* imp, int32_t* sub, cudaStream_t s);
+void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32_t* str, const int32_t* rank,
+                           int hw, double* e1, uint8_t* hcnt, uint32_t* hop, uint8_t* imp, int32_t* sub,
+                           cudaStream_t s);
 
 // ---- kernels.cu: standalone (non-persistent) kernels ------------------------
-int hx_rows_per_tile(int nup, int ndn);
+int hx_rows_per_tile(int nup, int ndn, int hw_dn);
 void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s);
 // Deterministic dot product: result written to *out (device).  partials needs
 // dot_partials_size() doubles.
@@ -58,10 +58,11 @@ void launch_cf(const CFJob* jobs_dev, int njobs, const double* omega, int nw, cu
 enum LzMode { LZ_COEFF = 0, LZ_EIGVEC = 1 };
 enum LzInit { LZ_INIT_HASH = 0, LZ_INIT_APPLYC = 1, LZ_INIT_COPY = 2 };
 
+// The Lanczos vectors of a run live as interleaved (y, w) pairs: y_k = H w_k
+// - b_k w_{k-1} and w_k, read and written together (one 16-byte access).
 struct LzJob {
     DevSector S;
-    double* Y[2];
-    double* W[2];
+    double2* YW[2];       // ping-pong pair buffers [dim]
     double* eig;          // EIGVEC: output eigenvector (unnormalised)
     const double* coeff;  // EIGVEC: ground eigenvector of the tridiagonal [nstep]
     double* a;            // [maxnstep]
@@ -69,14 +70,16 @@ struct LzJob {
     int maxnstep;         // COEFF: LanczosSteps; EIGVEC: nstep of the coefficient pass
     int mode;
     int init;
-    int rows_per_tile;
-    int ntiles;
-    int npart;            // participating CTAs = min(grid, ntiles)
-    long long tile0;      // first tile of this job in the global tile list
-    long long slot0;      // first partial-sum slot
+    int rmax;             // rows per shared-memory chunk
+    int first_cta;        // first CTA whose element range meets this job
+    int npart;            // number of CTAs whose element range meets this job
+    int nspan;            // last - first + 1 such CTA: when the job has fewer elements than
+                          // the grid has CTAs the participants are not contiguous
+    int pad2;
+    long long slot0;      // first of the job's nspan partial-sum slots (slot = CTA - first_cta)
     uint64_t key;         // LZ_INIT_HASH
     ApplyCArgs ac;        // LZ_INIT_APPLYC
-    const double* ac_src; // LZ_INIT_APPLYC: source vector (the ground state); LZ_INIT_COPY: start vector
+    const double* src;    // LZ_INIT_APPLYC: the ground state; LZ_INIT_COPY: the start vector
 };
 
 struct LzState {
@@ -94,19 +97,28 @@ struct LzBatch {
     int njobs;
     int grid;
     int block;
-    size_t smem;
-    long long total_tiles;
     int max_steps;
     int max_eig_steps;
+    int pad;
+    size_t smem;
+    long long total_elems;  // sum of the jobs' dimensions: CTA b owns [b*E/G, (b+1)*E/G)
 };
 
-// Number of co-resident CTAs the persistent kernel gets for a given shared-memory size.
+// Element range of CTA b in a grid of G over E elements.
+inline long long lz_cta_lo(long long E, int G, int b) { return (long long)((__int128)E * b / G); }
+
+// Number of co-resident CTAs of the persistent kernel for a shared-memory size.
 int lz_grid_size(int device, size_t smem, int* block_out);
-// Runs the persistent kernel; jobs/state live on the device.  Returns a
-// cudaError_t; *dev_status receives the kernel's own status word.
 cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, LzState* state,
-                                      const long long* tile_prefix, double* partials,
+                                      const long long* elem_prefix, double* partials,
                                       unsigned* arrive, unsigned* sync_words, int* status,
                                       cudaStream_t s);
-size_t lz_smem_bytes(int nup, int rows_per_tile);
-int lz_rows_per_tile(int nup, int ndn);
+// Rows per shared-memory chunk for a sector and the shared memory it needs.
+int lz_rows_per_chunk(int nup, int ndn, int hw_dn, size_t budget);
+size_t lz_smem_bytes(int nup, int hw_dn, int rmax);
+size_t lz_smem_budget(int max_nup, int max_hw_dn);
+#ifdef EDZT_DEVICE_CHECKS
+int lz_debug_bad(long long* out4);
+int kernels_debug_bad(long long* out4);
+int tables_debug_bad(long long* out4);
+#endif

@@ -60,6 +60,22 @@ def solver(pkg):
     s.close()
 
 
+@pytest.fixture(autouse=True)
+def _device_checks(request):
+    """With a bounds-checked library build, fail a GPU test whose kernels recorded a bad index."""
+    yield
+    if "gpu" not in request.keywords:
+        return
+    L = sys.modules.get(PKG_NAME)
+    lib = getattr(L, "_lib", None) if L else None
+    if lib is None or not hasattr(lib, "edzt_debug_bad"):
+        return
+    import ctypes as C
+    bad = (C.c_longlong * 4)()
+    lib.edzt_debug_bad(bad)
+    assert bad[0] == 0, f"device bounds check {list(bad)}"
+
+
 def oracle_for(O, m):
     """CPU oracle of a package Model."""
     return O.Oracle(m.norb, m.nbath, m.em, m.ek, m.vmk, m.U, m.Up, m.Jex, m.Jp, m.mu)

@@ -33,15 +33,30 @@ def test_lanczos_iteration_coefficients(pkg, solver, oracle_mod, engine):
         m = random_model(pkg, rng, 1, 9, spin_dep=True)
         solver.set_model(m)
         o = oracle_for(oracle_mod, m)
-        for nu, nd in [(5, 5), (4, 6), (1, 1), (0, 1)]:
+        # large sectors (dim 63504, 52920): the first 50 coefficients
+        for nu, nd in [(5, 5), (4, 6)]:
             v0 = oracle_mod.start_vector(11, 0, o.dim(nu, nd))
             n_ref, a_ref, b_ref = o.lanczos_iteration(nu, nd, v0, 120)
             n, a, b = solver.lanczos_iteration(nu, nd, v0, 120)
             assert n == n_ref, (nu, nd)
             k = ab_compare_len(b_ref, n)
+            assert k == 50
             assert np.abs(a[:k] - a_ref[:k]).max() <= AB_TOL
             assert np.abs(b[:k] - b_ref[:k]).max() <= AB_TOL
             assert b[0] == 0.0
+        # small sectors (dim 100, 10): orthogonality is lost after a few tens
+        # of steps, so only the leading coefficients and the Ritz value compare
+        for nu, nd in [(1, 1), (0, 1)]:
+            v0 = oracle_mod.start_vector(11, 0, o.dim(nu, nd))
+            n_ref, a_ref, b_ref = o.lanczos_iteration(nu, nd, v0, 120)
+            n, a, b = solver.lanczos_iteration(nu, nd, v0, 120)
+            assert n == n_ref, (nu, nd)
+            k = min(ab_compare_len(b_ref, n), 8)
+            assert np.abs(a[:k] - a_ref[:k]).max() <= AB_TOL
+            assert np.abs(b[:k] - b_ref[:k]).max() <= AB_TOL
+            e, _ = oracle_mod.tridiag_lowest(a, b, n)
+            e_ref, _ = oracle_mod.tridiag_lowest(a_ref, b_ref, n_ref)
+            assert _e_ok(e, e_ref)
     finally:
         solver.set_engine(0)
 
@@ -104,7 +119,12 @@ def test_ground_state_and_green_bethe_n6(solver, bethe, engine):
         assert np.abs(cg["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
         c, cr = cg["coeffs"], cg_ref["coeffs"]
         for q in (0, 2):   # (a^+, b^+) and (a^-, b^-) of spin up
-            k = ab_compare_len(cr[0, 0, q + 1], cfg["maxnstep"])
+            # the excitation sectors have dimension 300 and c^+|gs> lives in a
+            # smaller symmetric subspace: orthogonality is lost within ~15 steps
+            # (the plain engine, which repeats the reference's arithmetic step
+            # by step, already differs from the oracle by 1e-7 at step 20), so
+            # only the leading 10 coefficients compare; G(i w) is checked above
+            k = min(10, ab_compare_len(cr[0, 0, q + 1], cfg["maxnstep"]))
             assert np.abs(c[0, 0, q, :k] - cr[0, 0, q, :k]).max() <= AB_TOL
             assert np.abs(c[0, 0, q + 1, :k] - cr[0, 0, q + 1, :k]).max() <= AB_TOL
         bp1, bm1 = c[0, 0, 1, 0], c[0, 0, 3, 0]
