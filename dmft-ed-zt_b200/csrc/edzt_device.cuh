@@ -15,15 +15,6 @@
 #define EDZT_MAX_P (1 << EDZT_MAX_NORB)
 #define EDZT_MAX_JT 12  // norb*(norb-1) spin-flip/pair-hop transitions per pattern pair
 
-// Packed hop word (kernel-side hopping tables): bits 0..19 the target
-// string's rank (C(20,10) < 2^20), bits 20..26 the index of the amplitude
-// V(a,l) in the spin's coefficient table, bit 31 the fermion sign.
-#define HOP_RANK_MASK 0xFFFFFu
-#define HOP_CIDX_SHIFT 20
-#define HOP_CIDX_MASK 0x7Fu
-#define HOP_SIGN 0x80000000u
-#define EDZT_MAX_COEF 128
-
 // One spin species of one sector: strings with a fixed electron count and
 // the per-string tables derived from the impurity model.
 struct DevSpin {
@@ -33,19 +24,11 @@ struct DevSpin {
     const int32_t* rank;    // [2^nsite] rank of a string, -1 if popcount != n
     const double* e1;       // [count] one-body energy: sum (em-mu) n_imp + sum ek n_bath
     const uint8_t* hcnt;    // [count] number of allowed impurity<->bath hops
-    const uint32_t* hop;    // [hw][count] packed hop words
-    const double* coef;     // [ncoef] amplitudes V(a,l) of this spin, index a*nbath + l
-    int ncoef;
-    int pad;
+    const int32_t* hidx;    // [hw][count] target rank of each hop
+    const double* hval;     // [hw][count] signed amplitude of each hop
     const uint8_t* imp;     // [count] impurity bits (sites 1..norb)
     const int32_t* sub;     // [count][P] rank after replacing the impurity bits (norb > 1)
 };
-
-__device__ __forceinline__ double hop_coef(uint32_t p, const double* coef)
-{
-    const double c = coef[(p >> HOP_CIDX_SHIFT) & HOP_CIDX_MASK];
-    return (p & HOP_SIGN) ? -c : c;
-}
 
 // Spin-flip / pair-hop transition between impurity patterns (pu, pd) -> (pu2, pd2).
 struct JTrans {

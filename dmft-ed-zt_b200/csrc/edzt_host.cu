@@ -158,7 +158,7 @@ struct StrTable {
 
 struct OpsTable {
     int hw = 0;
-    std::unique_ptr<DevBuf> e1, hcnt, hop, imp, sub;
+    std::unique_ptr<DevBuf> e1, hcnt, hidx, hval, imp, sub;
 };
 
 struct JHost {
@@ -179,7 +179,7 @@ struct edzt_ctx {
     bool has_j = false;
     std::map<int, std::unique_ptr<StrTable>> str_tables;
     std::map<std::pair<int, int>, std::unique_ptr<OpsTable>> ops_tables;
-    std::unique_ptr<DevBuf> wint, jcnt, jt, coef;
+    std::unique_ptr<DevBuf> wint, jcnt, jt;
     Pool pool;
     // resident ground state
     bool has_gs = false;
@@ -238,12 +238,14 @@ OpsTable& ops_table(edzt_ctx* c, int n, int sigma)
     const size_t cnt = (size_t)std::max(st.count, 1);
     t->e1 = std::make_unique<DevBuf>(sizeof(double) * cnt);
     t->hcnt = std::make_unique<DevBuf>(cnt);
-    t->hop = std::make_unique<DevBuf>(sizeof(uint32_t) * cnt * t->hw);
+    t->hidx = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * t->hw);
+    t->hval = std::make_unique<DevBuf>(sizeof(double) * cnt * t->hw);
     t->imp = std::make_unique<DevBuf>(cnt);
     if (c->has_j) t->sub = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * c->P);
     launch_build_spin_ops(c->model, sigma, st.count, st.str->as<uint32_t>(), st.rank->as<int32_t>(), t->hw,
-                          t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hop->as<uint32_t>(),
-                          t->imp->as<uint8_t>(), t->sub ? t->sub->as<int32_t>() : nullptr, c->stream);
+                          t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hidx->as<int32_t>(),
+                          t->hval->as<double>(), t->imp->as<uint8_t>(),
+                          t->sub ? t->sub->as<int32_t>() : nullptr, c->stream);
     g_launches += 1;
     CKLAUNCH();
     OpsTable& ref = *t;
@@ -276,15 +278,13 @@ DevSector make_sector(edzt_ctx* c, int nu, int nd)
         sp.rank = s.rank->as<int32_t>();
         sp.e1 = o.e1->as<double>();
         sp.hcnt = o.hcnt->as<uint8_t>();
-        sp.hop = o.hop->as<uint32_t>();
+        sp.hidx = o.hidx->as<int32_t>();
+        sp.hval = o.hval->as<double>();
         sp.imp = o.imp->as<uint8_t>();
         sp.sub = o.sub ? o.sub->as<int32_t>() : nullptr;
     };
     fill(S.up, su, ou);
     fill(S.dn, sd, od);
-    S.up.coef = c->coef->as<double>();
-    S.dn.coef = c->coef->as<double>() + EDZT_MAX_COEF;
-    S.up.ncoef = S.dn.ncoef = c->model.norb * c->model.nbath;
     S.dim = (long long)su.count * sd.count;
     S.P = c->P;
     S.has_j = c->has_j ? 1 : 0;
@@ -349,13 +349,6 @@ void build_model_tables(edzt_ctx* c)
             any_j = any_j || cnt > 0;
         }
     c->has_j = any_j;
-    // hop amplitudes V(a,l) per spin, the coefficient tables the packed hop words index
-    std::vector<double> cf(2 * EDZT_MAX_COEF, 0.0);
-    for (int sg = 0; sg < 2; sg++)
-        for (int a = 0; a < norb; a++)
-            for (int l = 0; l < m.nbath; l++) cf[sg * EDZT_MAX_COEF + a * m.nbath + l] = m.vmk[a][l][sg];
-    c->coef = std::make_unique<DevBuf>(sizeof(double) * cf.size());
-    CK(cudaMemcpy(c->coef->p, cf.data(), sizeof(double) * cf.size(), cudaMemcpyHostToDevice));
     c->wint = std::make_unique<DevBuf>(sizeof(double) * P * P);
     c->jcnt = std::make_unique<DevBuf>(sizeof(int) * P * P);
     c->jt = std::make_unique<DevBuf>(sizeof(JTrans) * jt.size());
@@ -448,21 +441,13 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     std::vector<LzJob> jobs(nj);
     std::vector<Lease<double2>> bufs;
     bufs.reserve((size_t)nj * 2);
-    int max_nup = 1, max_hw = 1;
+    size_t smem = 0;
+    int max_steps = 0;
     for (int j = 0; j < nj; j++) {
         JobSpec& s = specs[j];
         LzJob& J = jobs[j];
         std::memset(&J, 0, sizeof(J));
         J.S = make_sector(c, s.nu, s.nd);
-        max_nup = std::max(max_nup, J.S.up.count);
-        max_hw = std::max(max_hw, J.S.dn.hw);
-    }
-    // every job stages whole rows; the chunk height fills the same budget
-    const size_t budget = lz_smem_budget(max_nup, max_hw);
-    size_t smem = 0;
-    for (int j = 0; j < nj; j++) {
-        JobSpec& s = specs[j];
-        LzJob& J = jobs[j];
         const long long dim = J.S.dim;
         for (int q = 0; q < 2; q++) {
             bufs.emplace_back(c->pool, (size_t)dim);
@@ -478,8 +463,10 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
         J.key = s.key;
         J.ac = s.ac;
         J.src = s.ac_src;
-        J.rmax = lz_rows_per_chunk(J.S.up.count, J.S.dn.count, J.S.dn.hw, budget);
-        smem = std::max(smem, lz_smem_bytes(J.S.up.count, J.S.dn.hw, J.rmax));
+        J.rows = lz_rows_per_tile(J.S.up.count, J.S.dn.count, J.S.dn.hw);
+        J.ntiles = (J.S.dn.count + J.rows - 1) / J.rows;
+        smem = std::max(smem, lz_smem_bytes(J.S.up.count, J.S.dn.hw, J.rows));
+        max_steps = std::max(max_steps, J.maxnstep);
         if (s.mode == LZ_COEFF) {
             CK(cudaMemsetAsync(s.a, 0, sizeof(double) * s.maxnstep, c->stream));
             CK(cudaMemsetAsync(s.b, 0, sizeof(double) * s.maxnstep, c->stream));
@@ -488,71 +475,51 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     int block = 256;
     const int G = persistent_grid(c, smem, &block);
     if (G <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
-    // element partition: CTA b owns [lo(b), lo(b+1)) of the concatenated jobs
+    // tiles of all jobs in one list; CTA b takes tiles b, b+G, ...; the
+    // participants of job j are CTAs (tile0 + q) mod G, q < min(G, ntiles)
     std::vector<long long> prefix(nj + 1, 0);
-    for (int j = 0; j < nj; j++) prefix[j + 1] = prefix[j] + jobs[j].S.dim;
-    const long long E = prefix[nj];
-    for (int j = 0; j < nj; j++) { jobs[j].first_cta = -1; jobs[j].npart = 0; jobs[j].nspan = 0; }
-    {
-        int j = 0;
-        for (int b = 0; b < G; b++) {
-            const long long lo = lz_cta_lo(E, G, b), hi = lz_cta_lo(E, G, b + 1);
-            if (lo >= hi) continue;
-            while (j < nj && prefix[j + 1] <= lo) j++;
-            for (int q = j; q < nj && prefix[q] < hi; q++) {
-                if (jobs[q].first_cta < 0) jobs[q].first_cta = b;
-                jobs[q].npart++;
-                jobs[q].nspan = b - jobs[q].first_cta + 1;
-            }
-        }
-    }
     long long slots = 0;
-    int max_steps = 0, max_eig = 0, n_coeff = 0;
     for (int j = 0; j < nj; j++) {
         LzJob& J = jobs[j];
+        J.tile0 = prefix[j];
+        prefix[j + 1] = prefix[j] + J.ntiles;
+        J.npart = std::min(G, J.ntiles);
         J.slot0 = slots;
-        slots += J.nspan;
-        max_steps = std::max(max_steps, J.maxnstep);
-        if (J.mode == LZ_EIGVEC) max_eig = std::max(max_eig, J.maxnstep);
-        else n_coeff++;
+        slots += J.npart;
     }
-    std::vector<LzState> st(nj);
-    for (int j = 0; j < nj; j++) {
-        std::memset(&st[j], 0, sizeof(LzState));
-        st[j].active = 1;
-    }
-    // device-side batch description (one block of the pool)
-    const size_t bytes_jobs = sizeof(LzJob) * nj, bytes_st = sizeof(LzState) * nj;
-    const size_t bytes_pre = sizeof(long long) * (nj + 1), bytes_part = sizeof(double) * 3 * (size_t)slots;
-    const size_t bytes_arr = sizeof(unsigned) * nj;
+    std::vector<LzState> st(2 * (size_t)nj);
+    std::memset(st.data(), 0, sizeof(LzState) * st.size());
+    for (int j = 0; j < nj; j++) st[2 * (size_t)j].active = 1;
+    const size_t bytes_jobs = sizeof(LzJob) * nj, bytes_st = sizeof(LzState) * st.size();
+    const size_t bytes_pre = sizeof(long long) * (nj + 1), bytes_part = sizeof(double) * 8 * (size_t)slots;
+    const size_t bytes_sw = lz_sync_bytes(G);
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t total = al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part) + al(bytes_arr);
+    const size_t total = al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part) + al(bytes_sw);
     Lease<char> blob(c->pool, total);
     char* base = blob.p;
     LzJob* d_jobs = reinterpret_cast<LzJob*>(base);
     LzState* d_st = reinterpret_cast<LzState*>(base + al(bytes_jobs));
     long long* d_pre = reinterpret_cast<long long*>(base + al(bytes_jobs) + al(bytes_st));
     double* d_part = reinterpret_cast<double*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre));
-    unsigned* d_arr = reinterpret_cast<unsigned*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part));
+    unsigned* d_sw = reinterpret_cast<unsigned*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part));
+    std::vector<unsigned> sw(bytes_sw / sizeof(unsigned), 0u);
+    sw[64] = (unsigned)nj;   // runs still going
+    sw[96] = (unsigned)nj;   // its snapshot at the last barrier
     CK(cudaMemcpyAsync(d_jobs, jobs.data(), bytes_jobs, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(d_st, st.data(), bytes_st, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(d_pre, prefix.data(), bytes_pre, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(d_arr, 0, bytes_arr, c->stream));
-    unsigned sw[8] = {0, 0, (unsigned)n_coeff, 0, (unsigned)n_coeff, 0, 0, 0};
-    CK(cudaMemcpyAsync(c->sync_words->p, sw, sizeof(sw), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_sw, sw.data(), bytes_sw, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->status->p, 0, sizeof(int), c->stream));
     LzBatch B;
+    std::memset(&B, 0, sizeof(B));
     B.njobs = nj;
     B.grid = G;
     B.block = block;
     B.smem = smem;
-    B.total_elems = E;
-    B.pad = 0;
-    B.max_steps = max_steps;
-    B.max_eig_steps = max_eig;
+    B.total_tiles = prefix[nj];
+    B.max_passes = 2 * max_steps + 4;   // start vector, every step, and room for repeated steps
     CK(cudaEventRecord(c->ev0, c->stream));
-    CK(launch_lanczos_persistent(B, d_jobs, d_st, d_pre, d_part, d_arr, c->sync_words->as<unsigned>(),
-                                 c->status->as<int>(), c->stream));
+    CK(launch_lanczos_persistent(B, d_jobs, d_st, d_pre, d_part, d_sw, c->status->as<int>(), c->stream));
     CK(cudaEventRecord(c->ev1, c->stream));
     g_launches += 1;
     int status = 0;
@@ -564,8 +531,13 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     if (status != 0) throw EdztError{EDZT_ERR_CUDA, "persistent Lanczos kernel reported status " + std::to_string(status)};
     double bytes = 0.0;
     for (int j = 0; j < nj; j++) {
-        specs[j].nstep = (specs[j].mode == LZ_COEFF) ? st[j].nstep : specs[j].maxnstep;
-        specs[j].norm0 = st[j].norm0;
+        // the final state is the finished one of the two parity copies
+        const LzState& s0 = st[2 * (size_t)j];
+        const LzState& s1 = st[2 * (size_t)j + 1];
+        const LzState* fin = !s0.active ? &s0 : (!s1.active ? &s1 : nullptr);
+        if (!fin) throw EdztError{EDZT_ERR_NUMERIC, "Lanczos run did not finish within the pass limit"};
+        specs[j].nstep = fin->nstep;
+        specs[j].norm0 = fin->norm0;
         const double dim = (double)jobs[j].S.dim;
         const double init = (specs[j].init == LZ_INIT_HASH) ? 8.0 : 16.0;
         const double per_step = (specs[j].mode == LZ_COEFF) ? 24.0 : 40.0;

@@ -23,8 +23,8 @@ uint64_t edzt_binom(int n, int k);
 void launch_build_strings(int nsite, int n, uint32_t* str, int32_t* rank, cudaStream_t s);
 // Per-string tables of one spin species (sigma = 0 up, 1 down) for a model.
 void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32_t* str, const int32_t* rank,
-                           int hw, double* e1, uint8_t* hcnt, uint32_t* hop, uint8_t* imp, int32_t* sub,
-                           cudaStream_t s);
+                           int hw, double* e1, uint8_t* hcnt, int32_t* hidx, double* hval, uint8_t* imp,
+                           int32_t* sub, cudaStream_t s);
 
 // ---- kernels.cu: standalone (non-persistent) kernels ------------------------
 int hx_rows_per_tile(int nup, int ndn, int hw_dn);
@@ -65,30 +65,30 @@ struct LzJob {
     double2* YW[2];       // ping-pong pair buffers [dim]
     double* eig;          // EIGVEC: output eigenvector (unnormalised)
     const double* coeff;  // EIGVEC: ground eigenvector of the tridiagonal [nstep]
-    double* a;            // [maxnstep]
-    double* b;            // [maxnstep]
+    double* a;            // [maxnstep] a(1..), written as steps are accepted
+    double* b;            // [maxnstep] b(1..)
     int maxnstep;         // COEFF: LanczosSteps; EIGVEC: nstep of the coefficient pass
     int mode;
     int init;
-    int rmax;             // rows per shared-memory chunk
-    int first_cta;        // first CTA whose element range meets this job
-    int npart;            // number of CTAs whose element range meets this job
-    int nspan;            // last - first + 1 such CTA: when the job has fewer elements than
-                          // the grid has CTAs the participants are not contiguous
-    int pad2;
-    long long slot0;      // first of the job's nspan partial-sum slots (slot = CTA - first_cta)
+    int rows;             // rows per tile (full rows, staged in shared memory)
+    int ntiles;
+    int npart;            // participating CTAs = min(grid, ntiles)
+    long long tile0;      // first tile of this job in the global tile list
+    long long slot0;      // first of the job's npart partial-sum slots
     uint64_t key;         // LZ_INIT_HASH
     ApplyCArgs ac;        // LZ_INIT_APPLYC
     const double* src;    // LZ_INIT_APPLYC: the ground state; LZ_INIT_COPY: the start vector
 };
 
+// Recurrence state of one run between passes (every participating CTA
+// derives the same value; the first participant also stores it).
 struct LzState {
+    int k;                // step the pass computes (1-based); 0 before the first step
     int active;           // 1 while the run is going
     int nstep;            // result: number of valid Lanczos steps
-    int k;                // last completed step
-    int need_exact;       // 1: b_{k+1} is being summed exactly in an extra phase
-    double a_prev;        // a_k, used to form w_{k+1}
-    double b_cur;         // b_{k+1}, the next normaliser
+    int retry;            // the pass repeats step k with a corrected b_k
+    double a_prev;        // a_{k-1}
+    double b_cur;         // b_k, the normaliser of the step
     double norm0;         // ||v_init||
     double spare;
 };
@@ -97,26 +97,21 @@ struct LzBatch {
     int njobs;
     int grid;
     int block;
-    int max_steps;
-    int max_eig_steps;
-    int pad;
+    int max_passes;
     size_t smem;
-    long long total_elems;  // sum of the jobs' dimensions: CTA b owns [b*E/G, (b+1)*E/G)
+    long long total_tiles;
 };
 
-// Element range of CTA b in a grid of G over E elements.
-inline long long lz_cta_lo(long long E, int G, int b) { return (long long)((__int128)E * b / G); }
-
-// Number of co-resident CTAs of the persistent kernel for a shared-memory size.
 int lz_grid_size(int device, size_t smem, int* block_out);
+// state: [njobs][2] (pass parity); partials: [slots][2][4]
 cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, LzState* state,
-                                      const long long* elem_prefix, double* partials,
-                                      unsigned* arrive, unsigned* sync_words, int* status,
-                                      cudaStream_t s);
-// Rows per shared-memory chunk for a sector and the shared memory it needs.
-int lz_rows_per_chunk(int nup, int ndn, int hw_dn, size_t budget);
-size_t lz_smem_bytes(int nup, int hw_dn, int rmax);
-size_t lz_smem_budget(int max_nup, int max_hw_dn);
+                                      const long long* tile_prefix, double* partials,
+                                      unsigned* sync_words, int* status, cudaStream_t s);
+// Rows per tile and the shared memory a tile of that many rows needs.
+int lz_rows_per_tile(int nup, int ndn, int hw_dn);
+size_t lz_smem_bytes(int nup, int hw_dn, int rows);
+// Sync-word buffer size (bytes) for a grid of G CTAs.
+size_t lz_sync_bytes(int G);
 #ifdef EDZT_DEVICE_CHECKS
 int lz_debug_bad(long long* out4);
 int kernels_debug_bad(long long* out4);

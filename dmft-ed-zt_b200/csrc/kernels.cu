@@ -7,7 +7,7 @@
 
 static constexpr int kHxThreads = 256;
 static constexpr size_t kHxSmemTarget = 24 * 1024;
-static constexpr int kCoefDoubles = 2 * EDZT_MAX_COEF;
+static constexpr int kWintDoubles = EDZT_MAX_P * EDZT_MAX_P;
 
 #ifdef EDZT_DEVICE_CHECKS
 int kernels_debug_bad(long long* out4)
@@ -28,40 +28,33 @@ int hx_rows_per_tile(int nup, int ndn, int hw_dn)
 // ---------------------------------------------------------------------------
 // H.v: y = H x (accumulate = 0) or y = y + H x (accumulate = 1), the `py`
 // flag of src/impurity_hamiltonian.f90:241-245.  One CTA per block of R full
-// rows; the rows and their down-hop lists are staged in shared memory.
+// rows; the rows and their per-row hop data are staged in shared memory.
 // ---------------------------------------------------------------------------
 template <bool ACC>
 __global__ void __launch_bounds__(kHxThreads) k_hx(DevSector S, const double* __restrict__ x,
                                                    double* __restrict__ y, int R)
 {
     extern __shared__ double smem[];
-    double* cu = smem;
-    double* cd = smem + EDZT_MAX_COEF;
-    double* xs = smem + kCoefDoubles;
+    double* wint = smem;
     const int nup = S.up.count, ndn = S.dn.count;
+    Chunk C = chunk_layout(smem + kWintDoubles, R, nup, S.dn.hw);
     const int r0 = blockIdx.x * R;
     const int rows = min(R, ndn - r0);
-    uint32_t* dw = reinterpret_cast<uint32_t*>(xs + (size_t)R * nup);
-    int* dc = reinterpret_cast<int*>(dw + (size_t)R * S.dn.hw);
     const int n = rows * nup;
     const long long g0 = (long long)r0 * nup;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) xs[e] = __ldg(x + g0 + e);
-    stage_down_hops(S.dn, r0, rows, dw, dc);
-    stage_coefs(S, cu, cd);
+    for (int e = threadIdx.x; e < n; e += blockDim.x) C.xs[e] = __ldg(x + g0 + e);
+    stage_rows(S.dn, C, r0, rows);
+    stage_wint(S, wint);
     __syncthreads();
     auto fetch = [&](long long idx) {
         EDZT_OK_OR(idx >= 0 && idx < S.dim, 61, idx, S.dim, blockIdx.x, return 0.0)
         return __ldg(x + idx);
     };
-    int r = threadIdx.x / nup, iu = threadIdx.x - r * nup;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-        const int id = r0 + r;
-        double v = hv_element(S, iu, id, xs + r * nup, xs[e], dw + r * S.dn.hw, dc[r], cu, cd, fetch);
-        if (ACC) v = y[g0 + e] + v;
-        y[g0 + e] = v;
-        iu += blockDim.x;
-        while (iu >= nup) { iu -= nup; ++r; }
-    }
+    auto epi = [&](int r, int iu, double, double hv) {
+        const long long g = g0 + (long long)r * nup + iu;
+        y[g] = ACC ? y[g] + hv : hv;
+    };
+    for_column_items(C, [&](int iu, int ra, int rz) { hv_column(S, C, wint, iu, ra, rz, fetch, epi); });
 }
 
 void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s)
@@ -70,7 +63,7 @@ void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, c
     if (nup <= 0 || ndn <= 0) return;
     const int R = hx_rows_per_tile(nup, ndn, S.dn.hw);
     const int tiles = (ndn + R - 1) / R;
-    const size_t smem = kCoefDoubles * sizeof(double) + (size_t)R * staged_row_bytes(nup, S.dn.hw) + 16;
+    const size_t smem = kWintDoubles * sizeof(double) + (size_t)R * staged_row_bytes(nup, S.dn.hw) + 16;
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_hx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

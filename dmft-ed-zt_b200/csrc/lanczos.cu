@@ -2,64 +2,70 @@
 //
 // One cooperative launch runs every step of many independent Lanczos runs
 // ("jobs": sectors of the ground-state search, the eigenvector pass of the
-// winning sector, c / c^+ excitation runs of the Green's function).  The
-// jobs' elements are concatenated and CTA b owns the contiguous range
-// [b*E/G, (b+1)*E/G) in every phase, so the work is balanced to one element.
-// Phases are separated by a grid barrier with a bounded wait.
+// winning sector, c / c^+ excitation runs of the Green's function).  Each
+// job is cut into tiles of whole rows; the tiles of all jobs form one list
+// and CTA b takes tiles b, b+G, b+2G, ... in every pass, so the CTAs sweep
+// the vectors together (the rows a sweep gathers from stay in L2) and the
+// same CTAs meet the same job every pass.  Passes are separated by a
+// hierarchical grid barrier with a bounded wait.
 //
 // The recurrence is the reference's (src/lanczos_solver.f90:92-173):
-//   w_k = v_k / b_k,  y_k = H w_k - b_k w_{k-1},  a_k = <w_k, y_k>,
-//   v_{k+1} = y_k - a_k w_k,  b_{k+1} = ||v_{k+1}||.
-// Fusion: phase k stores the pair (y_k, w_k); the next phase forms
-// w_{k+1}(j) = (y_k(j) - a_k w_k(j)) * (1/b_{k+1}) wherever it reads it
-// (rows staged in shared memory for the up-spin hops, down-spin neighbours
-// gathered as one 16-byte pair per hop), so a step is one sweep.  The norm
-// needs a_k before it can be summed, so the pass sums around a predicted
-// shift instead: with t = y - a_{k-1} w it reduces <w,t>, <t,t>, <w,w>
-// together, then a_k = a_{k-1}<w,w> + <w,t> and, with d = a_k - a_{k-1},
-// b_{k+1}^2 = <t,t> - 2d<w,t> + d^2<w,w>.  The cancellation in that
-// difference scales with d^2/b^2 (consecutive a differ by O(b)) rather than
-// a^2/b^2.  When it is still too large (b^2 < 1e-2 <t,t>, e.g. an exhausted
-// Krylov space in a tiny sector) the step takes one extra phase that sums
-// (y - a w)^2 exactly, as the reference does.  The first step divides v_init by its norm exactly as the reference
-// does (w = v/|v|), so a one-dimensional sector breaks down with b(2) = 0.
-// Reductions are deterministic: per-CTA partials in fixed slots, summed in a
-// fixed order by the last CTA to finish each job.
+//   w_k = v_k / b_k,  v_k = y_{k-1} - a_{k-1} w_{k-1},
+//   y_k = H w_k - b_k w_{k-1},  a_k = <w_k, y_k>,  b_{k+1} = ||y_k - a_k w_k||.
+// Fusion: a pass stores the pair (y_k, w_k); the next pass forms w_{k+1}
+// wherever it reads it (rows staged in shared memory for the up-spin hops,
+// down-spin neighbours gathered as one 16-byte pair per hop), so a step is
+// one sweep.  Its sums are taken around the shift a_{k-1}: with
+// t = y - a_{k-1} w it reduces <w,t>, <t,t>, <w,w>, so a_k = a_{k-1}<w,w> +
+// <w,t> and, with d = a_k - a_{k-1}, b_{k+1}^2 = <t,t> - 2d<w,t> + d^2<w,w>.
+// The next pass, which forms v_{k+1} element by element anyway, also sums
+// ||v_{k+1}||^2 exactly; when that disagrees with the b_{k+1} it used (by
+// more than 1e-12 relative, e.g. in an exhausted Krylov space of a tiny
+// sector) the job repeats that step with the exact norm, as the reference
+// computes it.  The first step divides v_init by its norm exactly as the
+// reference does, so a one-dimensional sector breaks down with b(2) = 0.
+//
+// Between passes every participating CTA of a job re-derives the job's
+// scalars from the partial sums of the previous pass (slots in a fixed order,
+// so all of them get the same bits) and the first participant also stores
+// them; partial sums and states are double-buffered by pass parity, so no
+// per-job atomics are needed.
 #include <cuda_runtime.h>
+#include <type_traits>
 #include "edzt_internal.h"
 #include "hv_row.cuh"
 
 static constexpr int kLzThreads = 256;
-static constexpr size_t kLzSmemTarget = 24 * 1024;
-static constexpr double kExactFrac = 1.0e-2;
+// CTAs per SM the register allocation is sized for
+#ifndef EDZT_LZ_MINBLOCKS
+#define EDZT_LZ_MINBLOCKS 2
+#endif
+static constexpr size_t kLzTileTarget = 24 * 1024;
+static constexpr double kVerifyTol = 1.0e-12;
 static constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000ull * 1000ull * 1000ull;
-static constexpr int kFixedDoubles = 96 + 2 * EDZT_MAX_COEF;   // reduction scratch + amplitude tables
+static constexpr int kFixedDoubles = 128 + EDZT_MAX_P * EDZT_MAX_P;   // reduction scratch + wint
+static constexpr int kBarGroup = 16;                                  // CTAs per barrier group
 
-// sync words
-#define SW_COUNT 0
-#define SW_GEN 1
-#define SW_ACTIVE 2
-#define SW_EXACT 3
-#define SW_SNAP_ACTIVE 4
-#define SW_SNAP_EXACT 5
+// sync words (unsigned), each counter on its own 128-byte line
+#define SW_GEN 0
+#define SW_TOP 32
+#define SW_ACTIVE 64
+#define SW_SNAP 96
+#define SW_GROUP(g) (128 + 32 * (g))
 
-size_t lz_smem_budget(int max_nup, int max_hw_dn)
+size_t lz_sync_bytes(int G) { return sizeof(unsigned) * (128 + 32 * (size_t)((G + kBarGroup - 1) / kBarGroup)); }
+
+int lz_rows_per_tile(int nup, int ndn, int hw_dn)
 {
-    const size_t one = staged_row_bytes(max_nup, max_hw_dn);
-    return one > kLzSmemTarget ? one : kLzSmemTarget;
-}
-
-int lz_rows_per_chunk(int nup, int ndn, int hw_dn, size_t budget)
-{
-    int r = (int)(budget / staged_row_bytes(nup, hw_dn));
+    int r = (int)(kLzTileTarget / staged_row_bytes(nup, hw_dn));
     if (r < 1) r = 1;
     if (r > ndn) r = ndn;
     return r;
 }
 
-size_t lz_smem_bytes(int nup, int hw_dn, int rmax)
+size_t lz_smem_bytes(int nup, int hw_dn, int rows)
 {
-    return kFixedDoubles * sizeof(double) + (size_t)rmax * staged_row_bytes(nup, hw_dn) + 16;
+    return kFixedDoubles * sizeof(double) + (size_t)rows * staged_row_bytes(nup, hw_dn) + 16;
 }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns()
@@ -69,8 +75,10 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     return t;
 }
 
-// Grid-wide barrier with a bounded wait.  The last CTA to arrive snapshots
-// the job counters, so every CTA takes the same branch after the barrier.
+// Hierarchical grid barrier with a bounded wait: CTAs arrive on a counter of
+// their group of 16, the last of each group on the top counter, the last of
+// all snapshots the active-run counter and releases.  Returns false (and the
+// kernel stops) when the wait ran out or another CTA reported an error.
 __device__ bool grid_barrier(unsigned* sw, int* status)
 {
     __shared__ int s_ok;
@@ -78,12 +86,20 @@ __device__ bool grid_barrier(unsigned* sw, int* status)
     if (threadIdx.x == 0) {
         int ok = 1;
         const unsigned gen = ld_acquire_u32(sw + SW_GEN);
+        const int G = gridDim.x;
+        const int g = blockIdx.x / kBarGroup;
+        const int ngroups = (G + kBarGroup - 1) / kBarGroup;
+        const unsigned gsize = (unsigned)min(kBarGroup, G - g * kBarGroup);
         __threadfence();
-        const unsigned prev = atomicAdd(sw + SW_COUNT, 1u);
-        if (prev == gridDim.x - 1) {
-            atomicExch(sw + SW_COUNT, 0u);
-            atomicExch(sw + SW_SNAP_ACTIVE, atomicAdd(sw + SW_ACTIVE, 0u));
-            atomicExch(sw + SW_SNAP_EXACT, atomicAdd(sw + SW_EXACT, 0u));
+        bool last = false;
+        if (atomicAdd(sw + SW_GROUP(g), 1u) == gsize - 1u) {
+            atomicExch(sw + SW_GROUP(g), 0u);
+            __threadfence();
+            last = atomicAdd(sw + SW_TOP, 1u) == (unsigned)ngroups - 1u;
+        }
+        if (last) {
+            atomicExch(sw + SW_TOP, 0u);
+            atomicExch(sw + SW_SNAP, atomicAdd(sw + SW_ACTIVE, 0u));
             __threadfence();
             atomicAdd(sw + SW_GEN, 1u);
         } else {
@@ -96,7 +112,7 @@ __device__ bool grid_barrier(unsigned* sw, int* status)
                     ok = 0;
                     break;
                 }
-                __nanosleep(32);
+                __nanosleep(20);
             }
         }
         __threadfence();
@@ -106,290 +122,325 @@ __device__ bool grid_barrier(unsigned* sw, int* status)
     return s_ok != 0;
 }
 
-__device__ __forceinline__ int find_job(const long long* __restrict__ prefix, int njobs, long long e)
+__device__ __forceinline__ int find_job(const long long* __restrict__ prefix, int njobs, long long t)
 {
     int lo = 0, hi = njobs - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(prefix + mid) <= e) lo = mid; else hi = mid - 1;
+        if (__ldg(prefix + mid) <= t) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
 
-__device__ __forceinline__ long long cta_lo(long long E, int G, int b)
+// One element of H.v from a staged chunk: the up-hop list of iu is loaded
+// eight entries at a time and the down-hop gathers of the row four at a time,
+// so their loads are in flight together.
+template <class Fetch>
+__device__ __forceinline__ double hv_element(const DevSector& S, const Chunk& C, const double* __restrict__ wint,
+                                             int r, int iu, double xe, Fetch fetch)
 {
-    // floor(E * b / G) without 128-bit arithmetic on the device
-    const long long q = E / G, r = E % G;
-    return q * b + (r * b) / G;
+    const int nup = C.nup, P = S.P;
+    const int pu = __ldg(S.up.imp + iu);
+    double acc = (__ldg(S.up.e1 + iu) + C.de1[r] + wint[pu * P + C.dimp[r]]) * xe;
+    const double* __restrict__ xrow = C.xs + r * nup;
+    const int hu = __ldg(S.up.hcnt + iu);
+    const int* __restrict__ hidx = S.up.hidx + iu;
+    const double* __restrict__ hval = S.up.hval + iu;
+    for (int h0 = 0; h0 < hu; h0 += 4) {
+        int j[4];
+        double c[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const bool on = h0 + q < hu;
+            j[q] = on ? __ldg(hidx + (h0 + q) * nup) : 0;
+            c[q] = on ? __ldg(hval + (h0 + q) * nup) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            EDZT_OK_OR(j[q] >= 0 && j[q] < nup, 11, iu, h0 + q, j[q], continue)
+            acc = fma(c[q], xrow[j[q]], acc);
+        }
+    }
+    const int hd = C.dcnt[r];
+    EDZT_OK_OR(hd >= 0 && hd <= C.hw, 13, iu, r, hd, return acc)
+    const int* __restrict__ off = C.doff + r * C.hw;
+    const double* __restrict__ val = C.dval + r * C.hw;
+    for (int h0 = 0; h0 < hd; h0 += 4) {
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) v[q] = (h0 + q < hd) ? fetch(off[h0 + q] + iu) : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (h0 + q < hd) acc = fma(val[h0 + q], v[q], acc);
+    }
+    if (S.has_j) {                          // spin-flip, pair-hopping (impurity_hamiltonian.f90:179-226)
+        const int id = C.r0 + r;
+        const int pp = pu * P + C.dimp[r];
+        const int nj = __ldg(S.jcnt + pp);
+        for (int t = 0; t < nj; t++) {
+            const JTrans tr = S.jt[pp * EDZT_MAX_JT + t];
+            const int iu2 = __ldg(S.up.sub + iu * P + tr.pu2);
+            const int id2 = __ldg(S.dn.sub + id * P + tr.pd2);
+            EDZT_OK_OR(iu2 >= 0 && iu2 < nup && id2 >= 0 && id2 < S.dn.count, 15, iu2, id2, pp, continue)
+            acc = fma(tr.c, fetch(id2 * nup + iu2), acc);
+        }
+    }
+    return acc;
 }
 
 // ---------------------------------------------------------------------------
-// finishers: run by the last participating CTA of a job, thread 0 only
+// scalar recurrence between passes (same on every participating CTA)
 // ---------------------------------------------------------------------------
-__device__ void finish_init(const LzJob& J, LzState* st, unsigned* sw, double svv)
-{
-    const double nrm = sqrt(svv);
-    st->norm0 = nrm;
-    st->need_exact = 0;
-    if (!(nrm > 0.0)) {                     // zero start vector: nothing to do
-        st->active = 0;
-        st->nstep = 0;
-        if (J.mode == LZ_COEFF) atomicSub(sw + SW_ACTIVE, 1u);
-        return;
-    }
-    st->a_prev = 0.0;
-    st->b_cur = nrm;
-    st->k = 0;
-}
+struct Sums {
+    double wt, tt, ww, vv;
+};
 
-__device__ void end_run(LzState* st, unsigned* sw, int nstep)
+// State of the pass after `prev`, from the sums of the pass that used `prev`.
+// `out` marks the first participant: it stores a(k), b(k) as they are
+// accepted and counts finished runs.
+__device__ LzState advance(const LzJob& J, const LzState& prev, const Sums& s, bool out, unsigned* sw)
 {
-    st->active = 0;
-    st->nstep = nstep;
-    atomicSub(sw + SW_ACTIVE, 1u);
-}
-
-// b_{k+1} known: apply the reference's stopping rule (breakdown tested before
-// the next division, see the file header).
-__device__ void accept_b(const LzJob& J, LzState* st, unsigned* sw, int k, double bnext)
-{
-    if (bnext < 1.0e-16) {
-        J.b[k] = 0.0;
-        end_run(st, sw, k);
-        return;
+    LzState n = prev;
+    n.retry = 0;
+    if (!prev.active) return n;
+    auto finish = [&](int nstep) {
+        n.active = 0;
+        n.nstep = nstep;
+        if (out) atomicSub(sw + SW_ACTIVE, 1u);
+    };
+    if (prev.k == 0) {                                  // after the start-vector pass
+        const double nrm = sqrt(s.vv);
+        n.norm0 = nrm;
+        if (!(nrm > 0.0)) { finish(0); return n; }      // zero start vector
+        n.k = 1;
+        n.a_prev = 0.0;
+        n.b_cur = nrm;
+        return n;
     }
-    J.b[k] = bnext;
-    st->b_cur = bnext;
-}
-
-// ah: the shift the pass used (a_{k-1}, 0 at k = 1); swt = <w,t>, stt = <t,t>.
-__device__ void finish_step(const LzJob& J, LzState* st, unsigned* sw, int k, double ah, double swt, double stt,
-                            double sww)
-{
-    const double a = fma(ah, sww, swt);     // a(k) = <w, y>   (lanczos_solver.f90:134,159)
-    J.a[k - 1] = a;
-    if (k == 1) J.b[0] = 0.0;               // :135
-    st->k = k;
-    st->a_prev = a;
-    if (k >= J.maxnstep) {                  // :137-141, :161-164
-        end_run(st, sw, k);
-        return;
+    const int k = prev.k;
+    if (J.mode == LZ_EIGVEC) {                          // stored coefficients, no sums
+        if (k >= J.maxnstep) { finish(k); return n; }
+        n.k = k + 1;
+        n.a_prev = J.a[k - 1];
+        n.b_cur = J.b[k];
+        return n;
     }
+    if (k >= 2) {                                       // verify the b_k the step used
+        const double bex = sqrt(s.vv);
+        if (bex < 1.0e-16) {                            // breakdown (lanczos_solver.f90:161)
+            if (out) J.b[k - 1] = 0.0;
+            finish(k - 1);
+            return n;
+        }
+        if (!(fabs(bex - prev.b_cur) <= kVerifyTol * bex)) {
+            if (out) J.b[k - 1] = bex;
+            n.b_cur = bex;
+            n.retry = 1;
+            return n;
+        }
+    }
+    const double ah = (k == 1) ? 0.0 : prev.a_prev;
+    const double a = fma(ah, s.ww, s.wt);               // a(k) = <w, y>  (lanczos_solver.f90:134,159)
+    if (out) {
+        J.a[k - 1] = a;
+        if (k == 1) J.b[0] = 0.0;                       // :135
+    }
+    if (k >= J.maxnstep) { finish(k); return n; }       // :137-141, :161-164
     const double d = a - ah;
-    const double bb2 = stt - 2.0 * d * swt + d * d * sww;
-    if (bb2 > kExactFrac * stt) {
-        accept_b(J, st, sw, k, sqrt(bb2));
-    } else {                                // cancellation: sum (y - a w)^2 exactly next phase
-        st->need_exact = 1;
-        atomicAdd(sw + SW_EXACT, 1u);
-    }
-}
-
-__device__ void finish_exact(const LzJob& J, LzState* st, unsigned* sw, double svv)
-{
-    st->need_exact = 0;
-    atomicSub(sw + SW_EXACT, 1u);
-    accept_b(J, st, sw, st->k, sqrt(svv));
+    const double bb2 = s.tt - 2.0 * d * s.wt + d * d * s.ww;
+    // an ill-conditioned or non-positive estimate is repaired by the next
+    // pass's exact norm (one repeated step)
+    const double bn = sqrt(fmax(bb2, 1.0e-300));
+    if (out) J.b[k] = bn;
+    n.k = k + 1;
+    n.a_prev = a;
+    n.b_cur = bn;
+    return n;
 }
 
 // ---------------------------------------------------------------------------
 // the persistent kernel
 // ---------------------------------------------------------------------------
-enum { PH_INIT = 0, PH_STEP = 1, PH_EXACT = 2 };
-
-__global__ void __launch_bounds__(kLzThreads, 4) k_lanczos(LzBatch B, const LzJob* __restrict__ jobs,
-                                                           LzState* __restrict__ state,
-                                                           const long long* __restrict__ prefix,
-                                                           double* __restrict__ partials,
-                                                           unsigned* __restrict__ arrive,
-                                                           unsigned* __restrict__ sw, int* __restrict__ status)
+__global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
+    k_lanczos(LzBatch B, const LzJob* __restrict__ jobs, LzState* __restrict__ state,
+              const long long* __restrict__ prefix, double* __restrict__ partials, unsigned* __restrict__ sw,
+              int* __restrict__ status)
 {
     extern __shared__ double smem[];
-    double* red = smem;                                  // 96 doubles of reduction scratch
-    double* cu = smem + 96;                              // up-spin hop amplitudes
-    double* cd = cu + EDZT_MAX_COEF;                     // down-spin hop amplitudes
-    double* xs = smem + kFixedDoubles;                   // staged rows of w
+    double* red = smem;                                  // 128 doubles of reduction scratch
+    double* wint = smem + 128;                           // interaction energies by impurity patterns
+    double* chunk_base = smem + kFixedDoubles;           // staged rows of the current tile
     __shared__ LzJob sJ;
     __shared__ LzState sS;
-    __shared__ int s_last, s_run;
+    __shared__ int s_job, s_run;
 
     const int G = gridDim.x;
-    const long long E = B.total_elems;
-    const long long my_lo = cta_lo(E, G, blockIdx.x), my_hi = cta_lo(E, G, blockIdx.x + 1);
+    if (threadIdx.x == 0) s_job = -1;
+    __syncthreads();
 
-    auto load_job = [&](int j, bool coefs) {
-        __syncthreads();
-        const int* src = reinterpret_cast<const int*>(jobs + j);
-        int* dst = reinterpret_cast<int*>(&sJ);
-        for (int i = threadIdx.x; i < (int)(sizeof(LzJob) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
-        const int* ss = reinterpret_cast<const int*>(state + j);
-        int* sd = reinterpret_cast<int*>(&sS);
-        for (int i = threadIdx.x; i < (int)(sizeof(LzState) / sizeof(int)); i += blockDim.x) sd[i] = __ldcg(ss + i);
-        __syncthreads();
-        if (coefs) stage_coefs(sJ.S, cu, cd);
-    };
+    // slot of this CTA in the current job (participants: CTAs (tile0 + q) mod G, q < npart)
+    auto my_q = [&]() { return (int)(((long long)blockIdx.x - sJ.tile0 % G + G) % G); };
 
-    // Flush this CTA's partial sums of job j; the last participant reduces them.
-    auto flush = [&](int j, int phase, int step, double (&acc)[3]) {
-        block_sum<3>(acc, red);
+    // Enter job j in pass `pass`: load it if needed and derive its state.
+    auto begin_job = [&](int j, int pass) {
+        __syncthreads();
+        if (j != s_job) {
+            const int* src = reinterpret_cast<const int*>(jobs + j);
+            int* dst = reinterpret_cast<int*>(&sJ);
+            for (int i = threadIdx.x; i < (int)(sizeof(LzJob) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
+            __syncthreads();
+            stage_wint(sJ.S, wint);
+            if (threadIdx.x == 0) s_job = j;
+        }
+        if (pass == 0) {
+            if (threadIdx.x == 0) {
+                const int* ss = reinterpret_cast<const int*>(state + 2 * (size_t)j);
+                int* sd = reinterpret_cast<int*>(&sS);
+                for (int i = 0; i < (int)(sizeof(LzState) / sizeof(int)); i++) sd[i] = __ldcg(ss + i);
+            }
+            __syncthreads();
+            return;
+        }
+        // sum the previous pass's slots in participant order
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        const int par = (pass - 1) & 1;
+        for (int i = threadIdx.x; i < sJ.npart; i += blockDim.x) {
+            const double* p = partials + ((sJ.slot0 + i) * 2 + par) * 4;
+            v[0] += __ldcg(p); v[1] += __ldcg(p + 1); v[2] += __ldcg(p + 2); v[3] += __ldcg(p + 3);
+        }
+        block_sum<4>(v, red);
         if (threadIdx.x == 0) {
-            const int q = (int)blockIdx.x - sJ.first_cta;
-            EDZT_OK_OR(q >= 0 && q < sJ.nspan, 24, blockIdx.x, sJ.first_cta, sJ.nspan, return)
-            double* slot = partials + (sJ.slot0 + q) * 3;
-            slot[0] = acc[0]; slot[1] = acc[1]; slot[2] = acc[2];
-            __threadfence();
-            const unsigned prev = atomicAdd(arrive + j, 1u);
-            s_last = (prev == (unsigned)sJ.npart - 1u);
-            if (s_last) {
-                atomicExch(arrive + j, 0u);
+            LzState prev;
+            const int* ss = reinterpret_cast<const int*>(state + 2 * (size_t)j + par);
+            int* sd = reinterpret_cast<int*>(&prev);
+            for (int i = 0; i < (int)(sizeof(LzState) / sizeof(int)); i++) sd[i] = __ldcg(ss + i);
+            const bool first = (my_q() == 0);
+            Sums s{v[0], v[1], v[2], v[3]};
+            sS = advance(sJ, prev, s, first, sw);
+            if (first) {
+                state[2 * (size_t)j + (pass & 1)] = sS;
                 __threadfence();
             }
         }
         __syncthreads();
-        if (!s_last) return;
-        // sum the slots of the CTAs of the span that own elements, in CTA order
-        double v[3] = {0.0, 0.0, 0.0};
-        for (int i = threadIdx.x; i < sJ.nspan; i += blockDim.x) {
-            const int b = sJ.first_cta + i;
-            if (cta_lo(E, G, b) >= cta_lo(E, G, b + 1)) continue;
-            const double* p = partials + (sJ.slot0 + i) * 3;
-            v[0] += __ldcg(p); v[1] += __ldcg(p + 1); v[2] += __ldcg(p + 2);
-        }
-        block_sum<3>(v, red);
+    };
+
+    auto flush = [&](int pass, double (&acc)[4]) {
+        block_sum<4>(acc, red);
         if (threadIdx.x == 0) {
-            LzState* st = state + j;
-            if (phase == PH_INIT) finish_init(sJ, st, sw, v[1]);
-            else if (phase == PH_STEP) finish_step(sJ, st, sw, step, step == 1 ? 0.0 : sS.a_prev, v[0], v[1], v[2]);
-            else finish_exact(sJ, st, sw, v[1]);
-            __threadfence();
+            EDZT_OK_OR(my_q() < sJ.npart, 24, blockIdx.x, sJ.tile0, sJ.npart, return)
+            double* p = partials + ((sJ.slot0 + my_q()) * 2 + (pass & 1)) * 4;
+            p[0] = acc[0]; p[1] = acc[1]; p[2] = acc[2]; p[3] = acc[3];
+        }
+    };
+
+    // Start vector rows of tile tl: materialise (v, 0) pairs, sum v^2.
+    auto init_tile = [&](int tl, double (&acc)[4]) {
+        const int nup = sJ.S.up.count;
+        const int r0 = tl * sJ.rows, rows = min(sJ.rows, sJ.S.dn.count - r0);
+        const long long g0 = (long long)r0 * nup, n = (long long)rows * nup;
+        double2* Y1 = sJ.YW[1];
+        for (long long e = threadIdx.x; e < n; e += blockDim.x) {
+            const long long g = g0 + e;
+            EDZT_OK_OR(g < sJ.S.dim, 25, g, sJ.S.dim, tl, break)
+            double v;
+            if (sJ.init == LZ_INIT_HASH) v = edzt_u01(sJ.key, (uint64_t)g);
+            else if (sJ.init == LZ_INIT_APPLYC) v = apply_c_value(sJ.ac, sJ.src, g);
+            else v = __ldg(sJ.src + g);
+            __stcg(Y1 + g, make_double2(v, 0.0));
+            acc[3] = fma(v, v, acc[3]);
+        }
+    };
+
+    // One Lanczos step (k = sS.k) on the rows of tile tl.  The first step
+    // (FIRST) divides by the start vector's norm exactly; later steps
+    // multiply by 1/b_k, so no division sits in their loops.
+    auto step_tile = [&](auto first_tag, int tl, double (&acc)[4]) {
+        constexpr bool FIRST = decltype(first_tag)::value;
+        const int nup = sJ.S.up.count, hwd = sJ.S.dn.hw;
+        const int k = sS.k;
+        const int p = k & 1;
+        const double2* __restrict__ YWp = sJ.YW[p];
+        double2* __restrict__ YWn = sJ.YW[p ^ 1];
+        const double b_cur = sS.b_cur, rb = 1.0 / b_cur, am = -sS.a_prev, mb = -b_cur;
+        const bool coeff = (sJ.mode == LZ_COEFF);
+        const double ck = coeff ? 0.0 : sJ.coeff[k - 1];
+        auto fetch = [&](int idx) {
+            EDZT_OK_OR(idx >= 0 && idx < sJ.S.dim, 21, idx, sJ.S.dim, k, return 0.0)
+            const double2 pr = __ldcg(YWp + idx);
+            if (FIRST) return pr.x / b_cur;
+            return fma(am, pr.y, pr.x) * rb;
+        };
+        const int r0 = tl * sJ.rows, rows = min(sJ.rows, sJ.S.dn.count - r0);
+        Chunk C = chunk_layout(chunk_base, sJ.rows, nup, hwd);
+        const int n = rows * nup;
+        EDZT_OK_OR(rows >= 1 && (long long)r0 * nup + n <= sJ.S.dim, 22, r0, rows, n, return)
+        const double2* __restrict__ Yt = YWp + (long long)r0 * nup;
+        double2* __restrict__ Ot = YWn + (long long)r0 * nup;
+        double* __restrict__ Et = coeff ? nullptr : sJ.eig + (long long)r0 * nup;
+        for (int e0 = threadIdx.x; e0 < n; e0 += 4 * blockDim.x) {
+            double2 pr[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int e = e0 + q * blockDim.x;
+                pr[q] = (e < n) ? __ldcg(Yt + e) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int e = e0 + q * blockDim.x;
+                if (e >= n) break;
+                if (FIRST) {
+                    C.xs[e] = pr[q].x / b_cur;
+                } else {
+                    const double v = fma(am, pr[q].y, pr[q].x);
+                    acc[3] = fma(v, v, acc[3]);      // exact ||v_k||^2: verifies b_k
+                    C.xs[e] = v * rb;
+                }
+            }
+        }
+        stage_rows(sJ.S.dn, C, r0, rows);
+        __syncthreads();
+        int r = threadIdx.x / nup, iu = threadIdx.x - r * nup;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            const double xe = C.xs[e];
+            const double hv = hv_element(sJ.S, C, wint, r, iu, xe, fetch);
+            const double y = FIRST ? hv : fma(mb, __ldcg(Yt + e).y, hv);
+            __stcg(Ot + e, make_double2(y, xe));
+            if (coeff) {
+                const double t = fma(am, xe, y);         // y - a_{k-1} w (a_0 = 0)
+                acc[0] = fma(xe, t, acc[0]);
+                acc[1] = fma(t, t, acc[1]);
+                acc[2] = fma(xe, xe, acc[2]);
+            } else {
+                __stcg(Et + e, FIRST ? ck * xe : fma(ck, xe, __ldcg(Et + e)));
+            }
+            iu += blockDim.x;
+            while (iu >= nup) { iu -= nup; ++r; }
         }
         __syncthreads();
     };
 
-    // One Lanczos step of the current job over its local elements [lo, hi).
-    auto step_range = [&](long long lo, long long hi, int step, double (&acc)[3]) {
-        const int nup = sJ.S.up.count, hwd = sJ.S.dn.hw;
-        const int p = step & 1;
-        const double2* YWp = sJ.YW[p];
-        double2* YWn = sJ.YW[p ^ 1];
-        double a_prev, b_cur;
-        if (sJ.mode == LZ_COEFF) { a_prev = sS.a_prev; b_cur = sS.b_cur; }
-        else {
-            a_prev = (step >= 2) ? sJ.a[step - 2] : 0.0;
-            b_cur = (step >= 2) ? sJ.b[step - 1] : sS.norm0;
-        }
-        const double rb = 1.0 / b_cur, am = -a_prev, mb = -b_cur;
-        const bool first = (step == 1);
-        const double ah = first ? 0.0 : am;                 // minus the predicted shift
-        const double ck = (sJ.mode == LZ_EIGVEC) ? sJ.coeff[step - 1] : 0.0;
-        auto wval = [&](double2 pr) { return first ? pr.x / b_cur : fma(am, pr.y, pr.x) * rb; };
-        auto fetch = [&](long long idx) {
-            EDZT_OK_OR(idx >= 0 && idx < sJ.S.dim, 21, idx, sJ.S.dim, step, return 0.0)
-            return wval(__ldcg(YWp + idx));
-        };
-        const int rmax = sJ.rmax;
-        uint32_t* dw = reinterpret_cast<uint32_t*>(xs + (size_t)rmax * nup);
-        int* dc = reinterpret_cast<int*>(dw + (size_t)rmax * hwd);
-        const int ra = (int)(lo / nup), rend = (int)((hi - 1) / nup) + 1;
-        for (int r0 = ra; r0 < rend; r0 += rmax) {
-            const int r1 = min(r0 + rmax, rend);
-            const long long g0 = (long long)r0 * nup;
-            const int nst = (r1 - r0) * nup;
-            EDZT_OK_OR(r1 - r0 <= rmax && r1 <= sJ.S.dn.count && g0 + nst <= sJ.S.dim, 22, r0, r1, rmax, break)
-            for (int e = threadIdx.x; e < nst; e += blockDim.x) xs[e] = wval(__ldcg(YWp + g0 + e));
-            stage_down_hops(sJ.S.dn, r0, r1 - r0, dw, dc);
-            __syncthreads();
-            const int c0 = (int)(max(lo, g0) - g0), c1 = (int)(min(hi, (long long)r1 * nup) - g0);
-            int el = c0 + threadIdx.x;
-            int r = el / nup, iu = el - r * nup;
-            for (; el < c1; el += blockDim.x) {
-                const long long g = g0 + el;
-                EDZT_OK_OR(r >= 0 && r < r1 - r0 && iu >= 0 && iu < nup && g < sJ.S.dim, 23, g, r, iu, break)
-                const double xe = xs[el];
-                const double hv = hv_element(sJ.S, iu, r0 + r, xs + (size_t)r * nup, xe, dw + (size_t)r * hwd,
-                                             dc[r], cu, cd, fetch);
-                const double y = first ? hv : fma(mb, __ldcg(YWp + g).y, hv);
-                __stcg(YWn + g, make_double2(y, xe));
-                if (sJ.mode == LZ_COEFF) {
-                    const double t = fma(ah, xe, y);         // y - a_{k-1} w
-                    acc[0] = fma(xe, t, acc[0]);
-                    acc[1] = fma(t, t, acc[1]);
-                    acc[2] = fma(xe, xe, acc[2]);
-                } else {
-                    double* eg = sJ.eig + g;
-                    __stcg(eg, first ? ck * xe : fma(ck, xe, __ldcg(eg)));
-                }
-                iu += blockDim.x;
-                while (iu >= nup) { iu -= nup; ++r; }
+    for (int pass = 0; pass < B.max_passes; pass++) {
+        int cur = -1;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (long long t = blockIdx.x; t < B.total_tiles; t += G) {
+            if (cur < 0 || t >= __ldg(prefix + cur + 1)) {
+                if (cur >= 0 && sS.active) flush(pass, acc);
+                cur = find_job(prefix, B.njobs, t);
+                begin_job(cur, pass);
+                acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
             }
-            __syncthreads();
+            if (!sS.active) continue;
+            const int tl = (int)(t - sJ.tile0);
+            if (pass == 0) init_tile(tl, acc);
+            else if (sS.k == 1) step_tile(std::true_type{}, tl, acc);
+            else step_tile(std::false_type{}, tl, acc);
         }
-    };
-
-    // One phase over this CTA's element range.
-    auto run_phase = [&](int phase, int step) {
-        if (my_lo >= my_hi) return;
-        int j = find_job(prefix, B.njobs, my_lo);
-        for (; j < B.njobs; j++) {
-            const long long pj = __ldg(prefix + j), pj1 = __ldg(prefix + j + 1);
-            if (pj >= my_hi) break;
-            load_job(j, phase == PH_STEP);
-            bool act, red_needed;
-            if (phase == PH_INIT) { act = true; red_needed = true; }
-            else if (phase == PH_EXACT) {
-                act = (sJ.mode == LZ_COEFF) && sS.active && sS.need_exact;
-                red_needed = true;
-            } else if (sJ.mode == LZ_COEFF) {
-                act = sS.active && !sS.need_exact;
-                red_needed = true;
-            } else {
-                act = sS.active && step <= sJ.maxnstep;
-                red_needed = false;
-            }
-            if (!act) continue;
-            const long long lo = max(my_lo, pj) - pj, hi = min(my_hi, pj1) - pj;
-            double acc[3] = {0.0, 0.0, 0.0};
-            if (phase == PH_INIT) {
-                double2* Y1 = sJ.YW[1];
-                for (long long g = lo + threadIdx.x; g < hi; g += blockDim.x) {
-                    EDZT_OK_OR(g < sJ.S.dim, 25, g, sJ.S.dim, j, break)
-                    double v;
-                    if (sJ.init == LZ_INIT_HASH) v = edzt_u01(sJ.key, (uint64_t)g);
-                    else if (sJ.init == LZ_INIT_APPLYC) v = apply_c_value(sJ.ac, sJ.src, g);
-                    else v = __ldg(sJ.src + g);
-                    __stcg(Y1 + g, make_double2(v, 0.0));
-                    acc[1] = fma(v, v, acc[1]);
-                }
-            } else if (phase == PH_EXACT) {
-                const double2* YWn = sJ.YW[(step & 1) ^ 1];
-                const double am = -sS.a_prev;
-                for (long long g = lo + threadIdx.x; g < hi; g += blockDim.x) {
-                    const double2 pr = __ldcg(YWn + g);
-                    const double v = fma(am, pr.y, pr.x);
-                    acc[1] = fma(v, v, acc[1]);
-                }
-            } else {
-                step_range(lo, hi, step, acc);
-            }
-            if (red_needed) flush(j, phase, step, acc);
-        }
-    };
-
-    run_phase(PH_INIT, 0);
-    if (!grid_barrier(sw, status)) return;
-    for (int step = 1; step <= B.max_steps; step++) {
-        if (threadIdx.x == 0)
-            s_run = (ld_acquire_u32(sw + SW_SNAP_ACTIVE) > 0u) || (step <= B.max_eig_steps);
+        if (cur >= 0 && sS.active) flush(pass, acc);
+        if (!grid_barrier(sw, status)) return;
+        if (threadIdx.x == 0) s_run = ld_acquire_u32(sw + SW_SNAP) > 0u;
         __syncthreads();
         if (!s_run) break;
-        run_phase(PH_STEP, step);
-        if (!grid_barrier(sw, status)) return;
-        if (threadIdx.x == 0) s_run = ld_acquire_u32(sw + SW_SNAP_EXACT) > 0u;
-        __syncthreads();
-        if (s_run) {
-            run_phase(PH_EXACT, step);
-            if (!grid_barrier(sw, status)) return;
-        }
     }
 }
 
@@ -414,12 +465,11 @@ int lz_grid_size(int device, size_t smem, int* block_out)
     return per_sm * nsm;
 }
 
-cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, LzState* state,
-                                      const long long* elem_prefix, double* partials, unsigned* arrive,
-                                      unsigned* sync_words, int* status, cudaStream_t s)
+cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, LzState* state, const long long* tile_prefix,
+                                      double* partials, unsigned* sync_words, int* status, cudaStream_t s)
 {
     LzBatch b = B;
-    void* args[] = {(void*)&b, (void*)&jobs, (void*)&state, (void*)&elem_prefix, (void*)&partials,
-                    (void*)&arrive, (void*)&sync_words, (void*)&status};
+    void* args[] = {(void*)&b, (void*)&jobs, (void*)&state, (void*)&tile_prefix, (void*)&partials,
+                    (void*)&sync_words, (void*)&status};
     return cudaLaunchCooperativeKernel((const void*)k_lanczos, dim3(B.grid), dim3(B.block), args, B.smem, s);
 }

@@ -89,12 +89,13 @@ __global__ void k_build_rank(int nsite, int n, int32_t* __restrict__ rank)
     if (s < (1u << nsite)) rank[s] = (__popc(s) == n) ? rank_colex(s) : -1;
 }
 
-// Per string of one spin species: one-body energy, packed hop list,
-// impurity bits and the rank of every impurity-pattern substitution.
+// Per string of one spin species: one-body energy, hop list, impurity bits
+// and the rank of every impurity-pattern substitution.
 __global__ void k_build_spin_ops(DevModel m, int sigma, int count, const uint32_t* __restrict__ str,
                                  const int32_t* __restrict__ rank, int hw, double* __restrict__ e1,
-                                 uint8_t* __restrict__ hcnt, uint32_t* __restrict__ hop,
-                                 uint8_t* __restrict__ imp, int32_t* __restrict__ sub)
+                                 uint8_t* __restrict__ hcnt, int32_t* __restrict__ hidx,
+                                 double* __restrict__ hval, uint8_t* __restrict__ imp,
+                                 int32_t* __restrict__ sub)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
@@ -111,21 +112,25 @@ __global__ void k_build_spin_ops(DevModel m, int sigma, int count, const uint32_
     int h = 0;
     for (int a = 0; a < norb; a++) {
         for (int l = 0; l < nbath; l++) {
-            if (fabs(m.vmk[a][l][sigma]) < 1.0e-16) continue;   // :148
+            const double v = m.vmk[a][l][sigma];
+            if (fabs(v) < 1.0e-16) continue;                    // :148
             const int i = a, j = norb + l;                       // i < j
             const uint32_t bi = (u >> i) & 1u, bj = (u >> j) & 1u;
             if (bi == bj) continue;
             // bits strictly between i and j; for bi == 1 the reference's
             // sgn() also counts bit i and subtracts, which cancels (:161-171)
             const uint32_t between = ((1u << j) - 1u) & ~((2u << i) - 1u);
-            const uint32_t neg = (__popc(u & between) & 1) ? HOP_SIGN : 0u;
             const uint32_t u2 = u ^ (1u << i) ^ (1u << j);
             EDZT_OK_OR(h < hw && rank[u2] >= 0, 51, t, h, u2, continue)
-            hop[(size_t)h * count + t] = (uint32_t)rank[u2] | ((uint32_t)(a * nbath + l) << HOP_CIDX_SHIFT) | neg;
+            hidx[(size_t)h * count + t] = rank[u2];
+            hval[(size_t)h * count + t] = (__popc(u & between) & 1) ? -v : v;
             ++h;
         }
     }
-    for (int q = h; q < hw; q++) hop[(size_t)q * count + t] = 0u;
+    for (int q = h; q < hw; q++) {
+        hidx[(size_t)q * count + t] = 0;
+        hval[(size_t)q * count + t] = 0.0;
+    }
     hcnt[t] = (uint8_t)h;
     const uint32_t P = 1u << norb;
     imp[t] = (uint8_t)(u & (P - 1u));
@@ -150,10 +155,10 @@ void launch_build_strings(int nsite, int n, uint32_t* str, int32_t* rank, cudaSt
 }
 
 void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32_t* str, const int32_t* rank,
-                           int hw, double* e1, uint8_t* hcnt, uint32_t* hop, uint8_t* imp, int32_t* sub,
-                           cudaStream_t s)
+                           int hw, double* e1, uint8_t* hcnt, int32_t* hidx, double* hval, uint8_t* imp,
+                           int32_t* sub, cudaStream_t s)
 {
     if (count <= 0) return;
-    k_build_spin_ops<<<(count + 127) / 128, 128, 0, s>>>(m, sigma, count, str, rank, hw, e1, hcnt, hop, imp,
-                                                        sub);
+    k_build_spin_ops<<<(count + 127) / 128, 128, 0, s>>>(m, sigma, count, str, rank, hw, e1, hcnt, hidx, hval,
+                                                        imp, sub);
 }
