@@ -48,8 +48,11 @@ EXPORTS = (
     "edzt_set_engine", "edzt_basis", "edzt_basis_rank", "edzt_sector_dim", "edzt_hx", "edzt_apply_c",
     "edzt_lanczos_iteration", "edzt_diag_lanczos", "edzt_ground_state", "edzt_gs_dim",
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
-    "edzt_kernel_stats", "edzt_reset_stats",
+    "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc",
 )
+# Limits of edzt_lanczos_iteration_noalloc (its static scratch array).
+NOALLOC_MAX_DIM = 262144
+NOALLOC_MAX_STEPS = 2048
 
 
 class EDError(RuntimeError):
@@ -96,6 +99,7 @@ def load_library(path: str = LIB_PATH):
     L.edzt_hx.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp, C.c_int]
     L.edzt_apply_c.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_int, _vp]
     L.edzt_lanczos_iteration.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
+    L.edzt_lanczos_iteration_noalloc.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
     L.edzt_ground_state.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_uint64, _ip, _dp, _vp, _vp]
     L.edzt_gs_dim.argtypes = [_vp]
@@ -263,6 +267,18 @@ class Solver:
         n = C.c_int()
         self._check(self._L.edzt_lanczos_iteration(self._h, ne_up, ne_dn, _ptr(v_init), maxnstep, C.byref(n),
                                                    _ptr(a), _ptr(b)))
+        return n.value, a, b
+
+    def lanczos_iteration_noalloc(self, ne_up, ne_dn, v_init, maxnstep):
+        """lanczos_iteration from the library's static scratch array (no
+        device allocation; sector dim <= NOALLOC_MAX_DIM, maxnstep <=
+        NOALLOC_MAX_STEPS; the sector's tables must exist on the context)."""
+        v_init = _f64(v_init)
+        a = np.zeros(maxnstep)
+        b = np.zeros(maxnstep)
+        n = C.c_int()
+        self._check(self._L.edzt_lanczos_iteration_noalloc(self._h, ne_up, ne_dn, _ptr(v_init), maxnstep,
+                                                           C.byref(n), _ptr(a), _ptr(b)))
         return n.value, a, b
 
     def diag_lanczos(self, ne_up, ne_dn, maxnstep, seed=0, stream=0):

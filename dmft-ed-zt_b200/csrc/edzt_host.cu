@@ -1009,6 +1009,33 @@ int guarded(edzt_ctx* c, F&& f)
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// context accessors for the no-allocation entry point (noalloc.cu); none of
+// them builds a table or allocates
+// ---------------------------------------------------------------------------
+int edzt_ctx_device(const edzt_ctx* c) { return c->device; }
+
+cudaStream_t edzt_ctx_stream(const edzt_ctx* c) { return c->stream; }
+
+void edzt_ctx_set_error(edzt_ctx* c, const char* msg) { c->err = msg ? msg : ""; }
+
+void edzt_count_launches(long long n) { g_launches += n; }
+
+int edzt_ctx_ready_sector(edzt_ctx* c, int nu, int nd, DevSector* S, const char** why)
+{
+    if (!c->has_model) { *why = "no model: call edzt_set_model first"; return EDZT_ERR_STATE; }
+    if (!sector_valid(c, nu, nd)) { *why = "electron counts outside [0, nsite]"; return EDZT_ERR_ARG; }
+    const bool ready = c->str_tables.count(nu) && c->str_tables.count(nd) &&
+                       c->ops_tables.count(std::make_pair(nu, 0)) && c->ops_tables.count(std::make_pair(nd, 1));
+    if (!ready) {
+        *why = "the sector's tables are not built on this context: make one allocating call on the sector "
+               "first (edzt_hx or edzt_lanczos_iteration)";
+        return EDZT_ERR_STATE;
+    }
+    *S = make_sector(c, nu, nd);   // only looks the tables up
+    return EDZT_OK;
+}
+
 // ===========================================================================
 // C ABI
 // ===========================================================================

@@ -112,6 +112,16 @@ int lz_rows_per_tile(int nup, int ndn, int hw_dn);
 size_t lz_smem_bytes(int nup, int hw_dn, int rows);
 // Sync-word buffer size (bytes) for a grid of G CTAs.
 size_t lz_sync_bytes(int G);
+// ---- edzt_host.cu: context accessors (no table building, no allocation) -----
+struct edzt_ctx;
+int edzt_ctx_device(const edzt_ctx* c);
+cudaStream_t edzt_ctx_stream(const edzt_ctx* c);
+void edzt_ctx_set_error(edzt_ctx* c, const char* msg);
+void edzt_count_launches(long long n);
+// The sector of (nu, nd) when its tables already exist; else an error code
+// with the reason in *why.
+int edzt_ctx_ready_sector(edzt_ctx* c, int nu, int nd, DevSector* S, const char** why);
+
 #ifdef EDZT_DEVICE_CHECKS
 int lz_debug_bad(long long* out4);
 int kernels_debug_bad(long long* out4);

@@ -101,6 +101,26 @@ int edzt_apply_c(edzt_ctx *ctx, int ne_up, int ne_dn, const double *vec, int pm,
 int edzt_lanczos_iteration(edzt_ctx *ctx, int ne_up, int ne_dn, const double *v_init, int maxnstep,
                            int *nstep, double *a, double *b);
 
+/* edzt_lanczos_iteration without any device allocation.  No counterpart in
+ * the reference (its lanczos_iteration allocates its work vectors on every
+ * call).  For callers that cannot call cudaMalloc/cudaFree: device memory
+ * owned entirely by another allocator, or a latency-critical loop that must
+ * not take the device-wide synchronisation an allocation can cause.  Same
+ * arguments and results as edzt_lanczos_iteration, always on the persistent
+ * kernel, whose scratch is one static device array of about 8.2 MiB that
+ * every GPU loading the library holds until exit.  Limits: sector dimension
+ * <= EDZT_NOALLOC_MAX_DIM, maxnstep <= EDZT_NOALLOC_MAX_STEPS (EDZT_ERR_ARG
+ * beyond).  The sector's tables must already exist on the context (built by
+ * any earlier allocating call on that sector after edzt_set_model, e.g.
+ * edzt_hx or edzt_lanczos_iteration), else EDZT_ERR_STATE.  The first call
+ * on each device looks the scratch array up with that device current and
+ * should come before any stream capture.  The array is shared by all
+ * contexts of a device: calls whose GPU work overlaps race. */
+#define EDZT_NOALLOC_MAX_DIM 262144
+#define EDZT_NOALLOC_MAX_STEPS 2048
+int edzt_lanczos_iteration_noalloc(edzt_ctx *ctx, int ne_up, int ne_dn, const double *v_init, int maxnstep,
+                                   int *nstep, double *a, double *b);
+
 /* diag_lanczos (src/lanczos_solver.f90:20-90) with a reproducible start
  * vector (U[0,1) from (seed, stream)): lowest eigenvalue of the sector, its
  * eigenvector (nullable) and the residual |H g - E g|^2 (nullable). */
