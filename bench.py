@@ -138,6 +138,20 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU legs (the oracle: test infrastructure, used here only as the baseline)
 # ---------------------------------------------------------------------------
+def read_traffic(path):
+    """DRAM bytes per k_lanczos launch (dram__bytes_read.sum + dram__bytes_write.sum
+    from one ncu capture of this workload), from the `bytes_per_launch:` line of
+    the committed profile summary; None when there is none."""
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
 def cpu_solve_sample(cfg, threads=None):
     """Times the oracle on a bounded sample and extrapolates to one full solve.
 
@@ -334,12 +348,7 @@ def run_gpu(args):
                 "note": "24 B/state per coefficient step, 40 B/state per eigenvector step; the "
                         "ground-state batch (9 sectors, 245 MB of vectors) exceeds L2, the eigenvector "
                         "and Green's-function launches (<= 27 MB) are L2-resident"}
-    if os.path.exists(args.traffic_file):
-        try:
-            with open(args.traffic_file) as f:
-                roofline["traffic"] = json.load(f).get("bytes_per_launch")
-        except Exception:
-            pass
+    roofline["traffic"] = read_traffic(args.traffic_file)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -372,7 +381,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
-    ap.add_argument("--traffic-file", default=os.path.join(ROOT, "profiles", "k_lanczos_traffic.json"))
+    ap.add_argument("--traffic-file", default=os.path.join(ROOT, "profiles", "k_lanczos_aim_n12_dram.txt"))
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
