@@ -19,16 +19,28 @@
 // the per-string tables derived from the impurity model.
 struct DevSpin {
     int count;              // C(nsite, n)
-    int hw;                 // hop-table slot stride (slots per string, upper bound)
+    int hw;                 // packed hop slots per string: a multiple of 4, >= every string's hop count
+    int namp;               // amplitude slots: 2 * norb * nbath
     const uint32_t* str;    // [count] ascending bit strings (ed_basis.f90:94-112)
     const int32_t* rank;    // [2^nsite] rank of a string, -1 if popcount != n
     const double* e1;       // [count] one-body energy: sum (em-mu) n_imp + sum ek n_bath
     const uint8_t* hcnt;    // [count] number of allowed impurity<->bath hops
-    const int32_t* hidx;    // [hw][count] target rank of each hop
-    const double* hval;     // [hw][count] signed amplitude of each hop
+    const uint4* hpk;       // [hw/4][count] hops of a string, four per uint4: target rank | slot << 20
+    const double* amp;      // [namp] amplitude of a slot: +V at 2c, -V at 2c+1, c = iorb*nbath + jbath
     const uint8_t* imp;     // [count] impurity bits (sites 1..norb)
     const int32_t* sub;     // [count][P] rank after replacing the impurity bits (norb > 1)
 };
+
+// Packed hop entry: target rank in the low 20 bits (C(20,10) < 2^20), the
+// amplitude slot (sign folded in) above.
+#define EDZT_HOP_RANK_BITS 20
+#define EDZT_MAX_AMP (2 * EDZT_MAX_NORB * EDZT_MAX_NSITE)
+__host__ __device__ __forceinline__ uint32_t edzt_hop_pack(int rank, int slot)
+{
+    return (uint32_t)rank | ((uint32_t)slot << EDZT_HOP_RANK_BITS);
+}
+__device__ __forceinline__ int edzt_hop_rank(uint32_t e) { return (int)(e & ((1u << EDZT_HOP_RANK_BITS) - 1u)); }
+__device__ __forceinline__ int edzt_hop_slot(uint32_t e) { return (int)(e >> EDZT_HOP_RANK_BITS); }
 
 // Spin-flip / pair-hop transition between impurity patterns (pu, pd) -> (pu2, pd2).
 struct JTrans {

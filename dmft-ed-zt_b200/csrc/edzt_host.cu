@@ -157,8 +157,8 @@ struct StrTable {
 };
 
 struct OpsTable {
-    int hw = 0;
-    std::unique_ptr<DevBuf> e1, hcnt, hidx, hval, imp, sub;
+    int hw = 0, namp = 0;
+    std::unique_ptr<DevBuf> e1, hcnt, hpk, amp, imp, sub;
 };
 
 struct JHost {
@@ -230,22 +230,28 @@ OpsTable& ops_table(edzt_ctx* c, int n, int sigma)
     StrTable& st = str_table(c, n);
     auto t = std::make_unique<OpsTable>();
     const int norb = c->model.norb, nbath = c->model.nbath;
-    int hw = 0;
+    // hop slots per string: the largest hop count of any string, rounded up to whole uint4s
+    const int maxh = edzt_max_hops(c->model, sigma, n);
+    t->hw = std::max(4, (maxh + 3) / 4 * 4);
+    t->namp = std::max(2, 2 * norb * nbath);
+    std::vector<double> amp((size_t)t->namp, 0.0);
     for (int a = 0; a < norb; a++)
-        for (int l = 0; l < nbath; l++)
-            if (std::fabs(c->model.vmk[a][l][sigma]) >= 1.0e-16) hw++;
-    t->hw = std::max(hw, 1);
+        for (int l = 0; l < nbath; l++) {
+            amp[2 * (a * nbath + l)] = c->model.vmk[a][l][sigma];
+            amp[2 * (a * nbath + l) + 1] = -c->model.vmk[a][l][sigma];
+        }
     const size_t cnt = (size_t)std::max(st.count, 1);
     t->e1 = std::make_unique<DevBuf>(sizeof(double) * cnt);
     t->hcnt = std::make_unique<DevBuf>(cnt);
-    t->hidx = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * t->hw);
-    t->hval = std::make_unique<DevBuf>(sizeof(double) * cnt * t->hw);
+    t->hpk = std::make_unique<DevBuf>(sizeof(uint32_t) * cnt * t->hw);
+    t->amp = std::make_unique<DevBuf>(sizeof(double) * t->namp);
     t->imp = std::make_unique<DevBuf>(cnt);
     if (c->has_j) t->sub = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * c->P);
+    CK(cudaMemcpyAsync(t->amp->p, amp.data(), sizeof(double) * t->namp, cudaMemcpyHostToDevice, c->stream));
     launch_build_spin_ops(c->model, sigma, st.count, st.str->as<uint32_t>(), st.rank->as<int32_t>(), t->hw,
-                          t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hidx->as<int32_t>(),
-                          t->hval->as<double>(), t->imp->as<uint8_t>(),
-                          t->sub ? t->sub->as<int32_t>() : nullptr, c->stream);
+                          t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hpk->as<uint32_t>(),
+                          t->imp->as<uint8_t>(), t->sub ? t->sub->as<int32_t>() : nullptr, c->stream);
+    CK(cudaStreamSynchronize(c->stream));   // amp is a host temporary
     g_launches += 1;
     CKLAUNCH();
     OpsTable& ref = *t;
@@ -274,12 +280,13 @@ DevSector make_sector(edzt_ctx* c, int nu, int nd)
     auto fill = [&](DevSpin& sp, StrTable& s, OpsTable& o) {
         sp.count = s.count;
         sp.hw = o.hw;
+        sp.namp = o.namp;
         sp.str = s.str->as<uint32_t>();
         sp.rank = s.rank->as<int32_t>();
         sp.e1 = o.e1->as<double>();
         sp.hcnt = o.hcnt->as<uint8_t>();
-        sp.hidx = o.hidx->as<int32_t>();
-        sp.hval = o.hval->as<double>();
+        sp.hpk = o.hpk->as<uint4>();
+        sp.amp = o.amp->as<double>();
         sp.imp = o.imp->as<uint8_t>();
         sp.sub = o.sub ? o.sub->as<int32_t>() : nullptr;
     };
@@ -475,6 +482,11 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     int block = 256;
     const int G = persistent_grid(c, smem, &block);
     if (G <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
+    for (int j = 0; j < nj; j++) {   // fewer rows per tile where that evens a job out over the grid
+        LzJob& J = jobs[j];
+        J.rows = lz_rows_balanced(J.S.dn.count, J.rows, G);
+        J.ntiles = (J.S.dn.count + J.rows - 1) / J.rows;
+    }
     // tiles of all jobs in one list; CTA b takes tiles b, b+G, ...; the
     // participants of job j are CTAs (tile0 + q) mod G, q < min(G, ntiles)
     std::vector<long long> prefix(nj + 1, 0);

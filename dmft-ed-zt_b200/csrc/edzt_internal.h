@@ -22,9 +22,12 @@ uint64_t edzt_binom(int n, int k);
 // Fills str[C(nsite,n)] (ascending) and rank[2^nsite] on the device.
 void launch_build_strings(int nsite, int n, uint32_t* str, int32_t* rank, cudaStream_t s);
 // Per-string tables of one spin species (sigma = 0 up, 1 down) for a model.
+// hpk: [hw/4][count] uint4 (packed hop entries, see edzt_hop_pack).
 void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32_t* str, const int32_t* rank,
-                           int hw, double* e1, uint8_t* hcnt, int32_t* hidx, double* hval, uint8_t* imp,
-                           int32_t* sub, cudaStream_t s);
+                           int hw, double* e1, uint8_t* hcnt, uint32_t* hpk, uint8_t* imp, int32_t* sub,
+                           cudaStream_t s);
+// Largest number of allowed hops of any string with n electrons of spin sigma.
+int edzt_max_hops(const DevModel& m, int sigma, int n);
 
 // ---- kernels.cu: standalone (non-persistent) kernels ------------------------
 int hx_rows_per_tile(int nup, int ndn, int hw_dn);
@@ -109,6 +112,8 @@ cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, LzSta
                                       unsigned* sync_words, int* status, cudaStream_t s);
 // Rows per tile and the shared memory a tile of that many rows needs.
 int lz_rows_per_tile(int nup, int ndn, int hw_dn);
+// Rows per tile (<= rows_max) that spread a job of ndn rows evenly over G CTAs.
+int lz_rows_balanced(int ndn, int rows_max, int G);
 size_t lz_smem_bytes(int nup, int hw_dn, int rows);
 // Sync-word buffer size (bytes) for a grid of G CTAs.
 size_t lz_sync_bytes(int G);

@@ -8,6 +8,7 @@
 static constexpr int kHxThreads = 256;
 static constexpr size_t kHxSmemTarget = 24 * 1024;
 static constexpr int kWintDoubles = EDZT_MAX_P * EDZT_MAX_P;
+static constexpr int kAmpDoubles = EDZT_MAX_AMP;
 
 #ifdef EDZT_DEVICE_CHECKS
 int kernels_debug_bad(long long* out4)
@@ -34,10 +35,11 @@ template <bool ACC>
 __global__ void __launch_bounds__(kHxThreads) k_hx(DevSector S, const double* __restrict__ x,
                                                    double* __restrict__ y, int R)
 {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     double* wint = smem;
+    double* amp = smem + kWintDoubles;
     const int nup = S.up.count, ndn = S.dn.count;
-    Chunk C = chunk_layout(smem + kWintDoubles, R, nup, S.dn.hw);
+    Chunk C = chunk_layout(smem + kWintDoubles + kAmpDoubles, R, nup, S.dn.hw);
     const int r0 = blockIdx.x * R;
     const int rows = min(R, ndn - r0);
     const int n = rows * nup;
@@ -45,16 +47,24 @@ __global__ void __launch_bounds__(kHxThreads) k_hx(DevSector S, const double* __
     for (int e = threadIdx.x; e < n; e += blockDim.x) C.xs[e] = __ldg(x + g0 + e);
     stage_rows(S.dn, C, r0, rows);
     stage_wint(S, wint);
+    stage_amp(S.up, amp);
     __syncthreads();
     auto fetch = [&](long long idx) {
         EDZT_OK_OR(idx >= 0 && idx < S.dim, 61, idx, S.dim, blockIdx.x, return 0.0)
         return __ldg(x + idx);
     };
-    auto epi = [&](int r, int iu, double, double hv) {
-        const long long g = g0 + (long long)r * nup + iu;
-        y[g] = ACC ? y[g] + hv : hv;
-    };
-    for_column_items(C, [&](int iu, int ra, int rz) { hv_column(S, C, wint, iu, ra, rz, fetch, epi); });
+    const SrcVec src{x};
+    int r = threadIdx.x / nup, iu = threadIdx.x - r * nup;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        double du, dn;
+        hv_elem(S, C, wint, amp, src, r, iu, C.xs[e], du, dn);
+        double acc = du + dn;
+        if (S.has_j) acc = hv_exchange(S, C, r, iu, acc, fetch);
+        const long long g = g0 + e;
+        y[g] = ACC ? y[g] + acc : acc;
+        iu += blockDim.x;
+        while (iu >= nup) { iu -= nup; ++r; }
+    }
 }
 
 void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s)
@@ -63,7 +73,7 @@ void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, c
     if (nup <= 0 || ndn <= 0) return;
     const int R = hx_rows_per_tile(nup, ndn, S.dn.hw);
     const int tiles = (ndn + R - 1) / R;
-    const size_t smem = kWintDoubles * sizeof(double) + (size_t)R * staged_row_bytes(nup, S.dn.hw) + 16;
+    const size_t smem = (kWintDoubles + kAmpDoubles) * sizeof(double) + (size_t)R * staged_row_bytes(nup, S.dn.hw);
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_hx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -43,7 +43,7 @@ static constexpr int kLzThreads = 256;
 static constexpr size_t kLzTileTarget = 24 * 1024;
 static constexpr double kVerifyTol = 1.0e-12;
 static constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000ull * 1000ull * 1000ull;
-static constexpr int kFixedDoubles = 128 + EDZT_MAX_P * EDZT_MAX_P;   // reduction scratch + wint
+static constexpr int kFixedDoubles = 128 + EDZT_MAX_P * EDZT_MAX_P + EDZT_MAX_AMP;   // reduction scratch, wint, amp
 static constexpr int kBarGroup = 16;                                  // CTAs per barrier group
 
 // sync words (unsigned), each counter on its own 128-byte line
@@ -63,9 +63,23 @@ int lz_rows_per_tile(int nup, int ndn, int hw_dn)
     return r;
 }
 
+int lz_rows_balanced(int ndn, int rows_max, int G)
+{
+    // rows per tile <= rows_max minimising the rows one CTA sweeps when the
+    // job runs alone, ceil(tiles / G) * rows; ties go to fewer, larger tiles
+    int best = rows_max;
+    long long best_cost = -1;
+    for (int r = rows_max; r >= 1; r--) {
+        const long long tiles = (ndn + r - 1) / r;
+        const long long cost = ((tiles + G - 1) / G) * r;
+        if (best_cost < 0 || cost < best_cost) { best = r; best_cost = cost; }
+    }
+    return best;
+}
+
 size_t lz_smem_bytes(int nup, int hw_dn, int rows)
 {
-    return kFixedDoubles * sizeof(double) + (size_t)rows * staged_row_bytes(nup, hw_dn) + 16;
+    return kFixedDoubles * sizeof(double) + (size_t)rows * staged_row_bytes(nup, hw_dn);
 }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns()
@@ -130,62 +144,6 @@ __device__ __forceinline__ int find_job(const long long* __restrict__ prefix, in
         if (__ldg(prefix + mid) <= t) lo = mid; else hi = mid - 1;
     }
     return lo;
-}
-
-// One element of H.v from a staged chunk: the up-hop list of iu is loaded
-// eight entries at a time and the down-hop gathers of the row four at a time,
-// so their loads are in flight together.
-template <class Fetch>
-__device__ __forceinline__ double hv_element(const DevSector& S, const Chunk& C, const double* __restrict__ wint,
-                                             int r, int iu, double xe, Fetch fetch)
-{
-    const int nup = C.nup, P = S.P;
-    const int pu = __ldg(S.up.imp + iu);
-    double acc = (__ldg(S.up.e1 + iu) + C.de1[r] + wint[pu * P + C.dimp[r]]) * xe;
-    const double* __restrict__ xrow = C.xs + r * nup;
-    const int hu = __ldg(S.up.hcnt + iu);
-    const int* __restrict__ hidx = S.up.hidx + iu;
-    const double* __restrict__ hval = S.up.hval + iu;
-    for (int h0 = 0; h0 < hu; h0 += 4) {
-        int j[4];
-        double c[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const bool on = h0 + q < hu;
-            j[q] = on ? __ldg(hidx + (h0 + q) * nup) : 0;
-            c[q] = on ? __ldg(hval + (h0 + q) * nup) : 0.0;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            EDZT_OK_OR(j[q] >= 0 && j[q] < nup, 11, iu, h0 + q, j[q], continue)
-            acc = fma(c[q], xrow[j[q]], acc);
-        }
-    }
-    const int hd = C.dcnt[r];
-    EDZT_OK_OR(hd >= 0 && hd <= C.hw, 13, iu, r, hd, return acc)
-    const int* __restrict__ off = C.doff + r * C.hw;
-    const double* __restrict__ val = C.dval + r * C.hw;
-    for (int h0 = 0; h0 < hd; h0 += 4) {
-        double v[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) v[q] = (h0 + q < hd) ? fetch(off[h0 + q] + iu) : 0.0;
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-            if (h0 + q < hd) acc = fma(val[h0 + q], v[q], acc);
-    }
-    if (S.has_j) {                          // spin-flip, pair-hopping (impurity_hamiltonian.f90:179-226)
-        const int id = C.r0 + r;
-        const int pp = pu * P + C.dimp[r];
-        const int nj = __ldg(S.jcnt + pp);
-        for (int t = 0; t < nj; t++) {
-            const JTrans tr = S.jt[pp * EDZT_MAX_JT + t];
-            const int iu2 = __ldg(S.up.sub + iu * P + tr.pu2);
-            const int id2 = __ldg(S.dn.sub + id * P + tr.pd2);
-            EDZT_OK_OR(iu2 >= 0 && iu2 < nup && id2 >= 0 && id2 < S.dn.count, 15, iu2, id2, pp, continue)
-            acc = fma(tr.c, fetch(id2 * nup + iu2), acc);
-        }
-    }
-    return acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -266,9 +224,10 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
               const long long* __restrict__ prefix, double* __restrict__ partials, unsigned* __restrict__ sw,
               int* __restrict__ status)
 {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     double* red = smem;                                  // 128 doubles of reduction scratch
     double* wint = smem + 128;                           // interaction energies by impurity patterns
+    double* amp = wint + EDZT_MAX_P * EDZT_MAX_P;        // up-spin hop amplitudes by slot
     double* chunk_base = smem + kFixedDoubles;           // staged rows of the current tile
     __shared__ LzJob sJ;
     __shared__ LzState sS;
@@ -290,6 +249,7 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
             for (int i = threadIdx.x; i < (int)(sizeof(LzJob) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
             __syncthreads();
             stage_wint(sJ.S, wint);
+            stage_amp(sJ.S.up, amp);
             if (threadIdx.x == 0) s_job = j;
         }
         if (pass == 0) {
@@ -365,7 +325,7 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
         const double b_cur = sS.b_cur, rb = 1.0 / b_cur, am = -sS.a_prev, mb = -b_cur;
         const bool coeff = (sJ.mode == LZ_COEFF);
         const double ck = coeff ? 0.0 : sJ.coeff[k - 1];
-        auto fetch = [&](int idx) {
+        auto fetch = [&](long long idx) {
             EDZT_OK_OR(idx >= 0 && idx < sJ.S.dim, 21, idx, sJ.S.dim, k, return 0.0)
             const double2 pr = __ldcg(YWp + idx);
             if (FIRST) return pr.x / b_cur;
@@ -400,11 +360,16 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
         }
         stage_rows(sJ.S.dn, C, r0, rows);
         __syncthreads();
+        const SrcPairs src{YWp, am};
         int r = threadIdx.x / nup, iu = threadIdx.x - r * nup;
         for (int e = threadIdx.x; e < n; e += blockDim.x) {
             const double xe = C.xs[e];
-            const double hv = hv_element(sJ.S, C, wint, r, iu, xe, fetch);
-            const double y = FIRST ? hv : fma(mb, __ldcg(Yt + e).y, hv);
+            const double wprev = FIRST ? 0.0 : __ldcg(reinterpret_cast<const double*>(Yt + e) + 1);
+            double du, dv;
+            hv_elem(sJ.S, C, wint, amp, src, r, iu, xe, du, dv);
+            double hv = du + (FIRST ? dv / b_cur : dv * rb);     // sum c * w_k(id', iu)
+            if (sJ.S.has_j) hv = hv_exchange(sJ.S, C, r, iu, hv, fetch);
+            const double y = FIRST ? hv : fma(mb, wprev, hv);
             __stcg(Ot + e, make_double2(y, xe));
             if (coeff) {
                 const double t = fma(am, xe, y);         // y - a_{k-1} w (a_0 = 0)

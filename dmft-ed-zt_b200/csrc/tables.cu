@@ -8,6 +8,7 @@
 // sum_k C(p_k, k) (0-based here) and the r-th string is recovered greedily
 // from the top bit down.  The fermion signs of src/impurity_hamiltonian.f90:
 // 251-260 are popcounts of the bits strictly between the two sites.
+#include <cmath>
 #include <cstdio>
 #include <mutex>
 #include <set>
@@ -93,9 +94,8 @@ __global__ void k_build_rank(int nsite, int n, int32_t* __restrict__ rank)
 // and the rank of every impurity-pattern substitution.
 __global__ void k_build_spin_ops(DevModel m, int sigma, int count, const uint32_t* __restrict__ str,
                                  const int32_t* __restrict__ rank, int hw, double* __restrict__ e1,
-                                 uint8_t* __restrict__ hcnt, int32_t* __restrict__ hidx,
-                                 double* __restrict__ hval, uint8_t* __restrict__ imp,
-                                 int32_t* __restrict__ sub)
+                                 uint8_t* __restrict__ hcnt, uint32_t* __restrict__ hpk,
+                                 uint8_t* __restrict__ imp, int32_t* __restrict__ sub)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
@@ -108,7 +108,9 @@ __global__ void k_build_spin_ops(DevModel m, int sigma, int count, const uint32_
     for (int l = 0; l < nbath; l++)
         if ((u >> (norb + l)) & 1u) e += m.ek[l][sigma];
     e1[t] = e;
-    // hybridisation hops (impurity_hamiltonian.f90:146-174), loop order iorb, jbath
+    // hybridisation hops (impurity_hamiltonian.f90:146-174), loop order iorb, jbath;
+    // entry h of string t sits at uint32 index ((h/4)*count + t)*4 + h%4
+    auto slot_at = [&](int h) -> uint32_t& { return hpk[((size_t)(h >> 2) * count + t) * 4 + (h & 3)]; };
     int h = 0;
     for (int a = 0; a < norb; a++) {
         for (int l = 0; l < nbath; l++) {
@@ -122,15 +124,12 @@ __global__ void k_build_spin_ops(DevModel m, int sigma, int count, const uint32_
             const uint32_t between = ((1u << j) - 1u) & ~((2u << i) - 1u);
             const uint32_t u2 = u ^ (1u << i) ^ (1u << j);
             EDZT_OK_OR(h < hw && rank[u2] >= 0, 51, t, h, u2, continue)
-            hidx[(size_t)h * count + t] = rank[u2];
-            hval[(size_t)h * count + t] = (__popc(u & between) & 1) ? -v : v;
+            const int neg = __popc(u & between) & 1;
+            slot_at(h) = edzt_hop_pack(rank[u2], 2 * (a * nbath + l) + neg);
             ++h;
         }
     }
-    for (int q = h; q < hw; q++) {
-        hidx[(size_t)q * count + t] = 0;
-        hval[(size_t)q * count + t] = 0.0;
-    }
+    for (int q = h; q < hw; q++) slot_at(q) = 0u;
     hcnt[t] = (uint8_t)h;
     const uint32_t P = 1u << norb;
     imp[t] = (uint8_t)(u & (P - 1u));
@@ -155,10 +154,30 @@ void launch_build_strings(int nsite, int n, uint32_t* str, int32_t* rank, cudaSt
 }
 
 void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32_t* str, const int32_t* rank,
-                           int hw, double* e1, uint8_t* hcnt, int32_t* hidx, double* hval, uint8_t* imp,
-                           int32_t* sub, cudaStream_t s)
+                           int hw, double* e1, uint8_t* hcnt, uint32_t* hpk, uint8_t* imp, int32_t* sub,
+                           cudaStream_t s)
 {
     if (count <= 0) return;
-    k_build_spin_ops<<<(count + 127) / 128, 128, 0, s>>>(m, sigma, count, str, rank, hw, e1, hcnt, hidx, hval,
-                                                        imp, sub);
+    k_build_spin_ops<<<(count + 127) / 128, 128, 0, s>>>(m, sigma, count, str, rank, hw, e1, hcnt, hpk, imp, sub);
+}
+
+int edzt_max_hops(const DevModel& m, int sigma, int n)
+{
+    const int ns = m.nsite;
+    if (n < 0 || n > ns) return 0;
+    int best = 0;
+    // every string with popcount n (Gosper's hack; the empty and full strings directly)
+    uint64_t u = (n == 0) ? 0ull : ((1ull << n) - 1ull);
+    const uint64_t end = 1ull << ns;
+    while (u < end) {
+        int h = 0;
+        for (int a = 0; a < m.norb; a++)
+            for (int l = 0; l < m.nbath; l++)
+                if (std::fabs(m.vmk[a][l][sigma]) >= 1.0e-16 && (((u >> a) ^ (u >> (m.norb + l))) & 1ull)) h++;
+        if (h > best) best = h;
+        if (n == 0) break;
+        const uint64_t c = u & (0ull - u), r = u + c;
+        u = (((r ^ u) >> 2) / c) | r;
+    }
+    return best;
 }
