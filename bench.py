@@ -274,10 +274,8 @@ def run_gpu(args):
     launches = s.launch_count() - launches0
     ks = s.kernel_stats()
     total_ms = sum(lat)
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    replicas = importlib.import_module("dmft_ed_zt_b200.replicas")
+    total_ms = replicas.max_over_ranks(total_ms, dist, device="cuda")
     value = world * K / (total_ms / 1000.0)
 
     # ---- end to end through the C ABI with host buffers ---------------------
@@ -307,10 +305,7 @@ def run_gpu(args):
         solve_host()
         torch.cuda.synchronize()
         e2e_ms += 1000.0 * (time.perf_counter() - t0)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = replicas.max_over_ranks(e2e_ms, dist, device="cuda")
     gs_dim = int(L.edzt_gs_dim(s._h))
     h2d = (em.nbytes + ek.nbytes + vmk.nbytes + sec.nbytes + omega_h.nbytes)
     d2h = 8 * gs_dim + G_h.nbytes + coeffs_h.nbytes + es_h.nbytes + 8
