@@ -161,9 +161,16 @@ struct OpsTable {
     std::unique_ptr<DevBuf> e1, hcnt, hpk, amp, imp, sub;
 };
 
-struct JHost {
-    int cnt;
-    JTrans t[EDZT_MAX_JT];
+// The model-dependent tables of one impurity model: per-spin operator tables
+// by (electron count, spin) and the interaction tables.  The single-model
+// entry points use the context's own; a batch holds one per instance.
+struct ModelTables {
+    bool valid = false;
+    DevModel model{};
+    int P = 1;
+    bool has_j = false;
+    std::map<std::pair<int, int>, std::unique_ptr<OpsTable>> ops;
+    std::unique_ptr<DevBuf> wint, jcnt, jt;
 };
 
 }  // namespace
@@ -173,13 +180,9 @@ struct edzt_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     int engine = EDZT_ENGINE_FUSED;
-    bool has_model = false;
-    DevModel model{};
-    int P = 1;
-    bool has_j = false;
-    std::map<int, std::unique_ptr<StrTable>> str_tables;
-    std::map<std::pair<int, int>, std::unique_ptr<OpsTable>> ops_tables;
-    std::unique_ptr<DevBuf> wint, jcnt, jt;
+    ModelTables mt;                         // the model of the single-model entry points
+    // bit strings and rank tables by (nsite, electron count): model-independent, shared
+    std::map<std::pair<int, int>, std::unique_ptr<StrTable>> str_tables;
     Pool pool;
     // resident ground state
     bool has_gs = false;
@@ -202,14 +205,14 @@ struct edzt_ctx {
 
 namespace {
 
-int nsite_of(const edzt_ctx* c) { return c->model.nsite; }
+int nsite_of(const edzt_ctx* c) { return c->mt.model.nsite; }
 
-StrTable& str_table(edzt_ctx* c, int n)
+StrTable& str_table_ns(edzt_ctx* c, int ns, int n)
 {
-    auto it = c->str_tables.find(n);
+    const auto key = std::make_pair(ns, n);
+    auto it = c->str_tables.find(key);
     if (it != c->str_tables.end()) return *it->second;
     auto t = std::make_unique<StrTable>();
-    const int ns = nsite_of(c);
     t->n = n;
     t->count = (int)edzt_binom(ns, n);
     t->str = std::make_unique<DevBuf>(sizeof(uint32_t) * (size_t)std::max(t->count, 1));
@@ -218,71 +221,68 @@ StrTable& str_table(edzt_ctx* c, int n)
     g_launches += 2;
     CKLAUNCH();
     StrTable& ref = *t;
-    c->str_tables.emplace(n, std::move(t));
+    c->str_tables.emplace(key, std::move(t));
     return ref;
 }
 
-OpsTable& ops_table(edzt_ctx* c, int n, int sigma)
+StrTable& str_table(edzt_ctx* c, int n) { return str_table_ns(c, nsite_of(c), n); }
+
+OpsTable& ops_table_mt(edzt_ctx* c, ModelTables& mt, int n, int sigma)
 {
     auto key = std::make_pair(n, sigma);
-    auto it = c->ops_tables.find(key);
-    if (it != c->ops_tables.end()) return *it->second;
-    StrTable& st = str_table(c, n);
+    auto it = mt.ops.find(key);
+    if (it != mt.ops.end()) return *it->second;
+    StrTable& st = str_table_ns(c, mt.model.nsite, n);
     auto t = std::make_unique<OpsTable>();
-    const int norb = c->model.norb, nbath = c->model.nbath;
+    const int norb = mt.model.norb, nbath = mt.model.nbath;
     // hop slots per string: the largest hop count of any string, rounded up to whole uint4s
-    const int maxh = edzt_max_hops(c->model, sigma, n);
+    const int maxh = edzt_max_hops(mt.model, sigma, n);
     t->hw = std::max(4, (maxh + 3) / 4 * 4);
     t->namp = std::max(2, 2 * norb * nbath);
-    std::vector<double> amp((size_t)t->namp, 0.0);
-    for (int a = 0; a < norb; a++)
-        for (int l = 0; l < nbath; l++) {
-            amp[2 * (a * nbath + l)] = c->model.vmk[a][l][sigma];
-            amp[2 * (a * nbath + l) + 1] = -c->model.vmk[a][l][sigma];
-        }
     const size_t cnt = (size_t)std::max(st.count, 1);
     t->e1 = std::make_unique<DevBuf>(sizeof(double) * cnt);
     t->hcnt = std::make_unique<DevBuf>(cnt);
     t->hpk = std::make_unique<DevBuf>(sizeof(uint32_t) * cnt * t->hw);
     t->amp = std::make_unique<DevBuf>(sizeof(double) * t->namp);
     t->imp = std::make_unique<DevBuf>(cnt);
-    if (c->has_j) t->sub = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * c->P);
-    CK(cudaMemcpyAsync(t->amp->p, amp.data(), sizeof(double) * t->namp, cudaMemcpyHostToDevice, c->stream));
-    launch_build_spin_ops(c->model, sigma, st.count, st.str->as<uint32_t>(), st.rank->as<int32_t>(), t->hw,
+    if (mt.has_j) t->sub = std::make_unique<DevBuf>(sizeof(int32_t) * cnt * mt.P);
+    launch_build_spin_ops(mt.model, sigma, st.count, st.str->as<uint32_t>(), st.rank->as<int32_t>(), t->hw,
                           t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hpk->as<uint32_t>(),
-                          t->imp->as<uint8_t>(), t->sub ? t->sub->as<int32_t>() : nullptr, c->stream);
-    CK(cudaStreamSynchronize(c->stream));   // amp is a host temporary
+                          t->amp->as<double>(), t->imp->as<uint8_t>(), t->sub ? t->sub->as<int32_t>() : nullptr,
+                          c->stream);
     g_launches += 1;
     CKLAUNCH();
     OpsTable& ref = *t;
-    c->ops_tables.emplace(key, std::move(t));
+    mt.ops.emplace(key, std::move(t));
     return ref;
 }
 
-bool sector_valid(const edzt_ctx* c, int nu, int nd)
+bool sector_valid_ns(int ns, int nu, int nd) { return nu >= 0 && nd >= 0 && nu <= ns && nd <= ns; }
+
+long long sector_dim_ns(int ns, int nu, int nd)
 {
-    return nu >= 0 && nd >= 0 && nu <= c->model.nsite && nd <= c->model.nsite;
+    if (!sector_valid_ns(ns, nu, nd)) return 0;
+    return (long long)edzt_binom(ns, nu) * (long long)edzt_binom(ns, nd);
 }
 
-long long sector_dim(const edzt_ctx* c, int nu, int nd)
-{
-    if (!sector_valid(c, nu, nd)) return 0;
-    return (long long)edzt_binom(c->model.nsite, nu) * (long long)edzt_binom(c->model.nsite, nd);
-}
+bool sector_valid(const edzt_ctx* c, int nu, int nd) { return sector_valid_ns(nsite_of(c), nu, nd); }
 
-DevSector make_sector(edzt_ctx* c, int nu, int nd)
+long long sector_dim(const edzt_ctx* c, int nu, int nd) { return sector_dim_ns(nsite_of(c), nu, nd); }
+
+DevSector make_sector_mt(edzt_ctx* c, ModelTables& mt, int nu, int nd)
 {
     DevSector S{};
-    StrTable& su = str_table(c, nu);
-    StrTable& sd = str_table(c, nd);
-    OpsTable& ou = ops_table(c, nu, 0);
-    OpsTable& od = ops_table(c, nd, 1);
-    auto fill = [&](DevSpin& sp, StrTable& s, OpsTable& o) {
-        sp.count = s.count;
+    const int ns = mt.model.nsite;
+    StrTable& su = str_table_ns(c, ns, nu);
+    StrTable& sd = str_table_ns(c, ns, nd);
+    OpsTable& ou = ops_table_mt(c, mt, nu, 0);
+    OpsTable& od = ops_table_mt(c, mt, nd, 1);
+    auto fill = [&](DevSpin& sp, StrTable& st, OpsTable& o) {
+        sp.count = st.count;
         sp.hw = o.hw;
         sp.namp = o.namp;
-        sp.str = s.str->as<uint32_t>();
-        sp.rank = s.rank->as<int32_t>();
+        sp.str = st.str->as<uint32_t>();
+        sp.rank = st.rank->as<int32_t>();
         sp.e1 = o.e1->as<double>();
         sp.hcnt = o.hcnt->as<uint8_t>();
         sp.hpk = o.hpk->as<uint4>();
@@ -293,22 +293,24 @@ DevSector make_sector(edzt_ctx* c, int nu, int nd)
     fill(S.up, su, ou);
     fill(S.dn, sd, od);
     S.dim = (long long)su.count * sd.count;
-    S.P = c->P;
-    S.has_j = c->has_j ? 1 : 0;
-    S.wint = c->wint->as<double>();
-    S.jcnt = c->jcnt->as<int>();
-    S.jt = c->jt->as<JTrans>();
+    S.P = mt.P;
+    S.has_j = mt.has_j ? 1 : 0;
+    S.wint = mt.wint->as<double>();
+    S.jcnt = mt.jcnt->as<int>();
+    S.jt = mt.jt->as<JTrans>();
     return S;
 }
+
+DevSector make_sector(edzt_ctx* c, int nu, int nd) { return make_sector_mt(c, c->mt, nu, nd); }
 
 // Interaction tables over impurity occupation patterns (pu, pd).
 // wint: impurity_hamiltonian.f90:119-141 without the em-mu terms (those are
 // one-body and live in e1).  Exchange transitions: :179-226.
-void build_model_tables(edzt_ctx* c)
+void build_model_tables(ModelTables& mt, cudaStream_t stream)
 {
-    const DevModel& m = c->model;
+    const DevModel& m = mt.model;
     const int norb = m.norb, P = 1 << norb;
-    c->P = P;
+    mt.P = P;
     std::vector<double> w(P * P, 0.0);
     std::vector<int> jc(P * P, 0);
     std::vector<JTrans> jt((size_t)P * P * EDZT_MAX_JT);
@@ -355,13 +357,41 @@ void build_model_tables(edzt_ctx* c)
             jc[pu * P + pd] = cnt;
             any_j = any_j || cnt > 0;
         }
-    c->has_j = any_j;
-    c->wint = std::make_unique<DevBuf>(sizeof(double) * P * P);
-    c->jcnt = std::make_unique<DevBuf>(sizeof(int) * P * P);
-    c->jt = std::make_unique<DevBuf>(sizeof(JTrans) * jt.size());
-    CK(cudaMemcpy(c->wint->p, w.data(), sizeof(double) * P * P, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->jcnt->p, jc.data(), sizeof(int) * P * P, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->jt->p, jt.data(), sizeof(JTrans) * jt.size(), cudaMemcpyHostToDevice));
+    mt.has_j = any_j;
+    mt.wint = std::make_unique<DevBuf>(sizeof(double) * P * P);
+    mt.jcnt = std::make_unique<DevBuf>(sizeof(int) * P * P);
+    mt.jt = std::make_unique<DevBuf>(sizeof(JTrans) * jt.size());
+    CK(cudaMemcpyAsync(mt.wint->p, w.data(), sizeof(double) * P * P, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(mt.jcnt->p, jc.data(), sizeof(int) * P * P, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(mt.jt->p, jt.data(), sizeof(JTrans) * jt.size(), cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));      // the host vectors go out of scope
+}
+
+// The reference's em(norb,2), ek(nbath,2), vmk(norb,nbath,2) (column-major) as a DevModel.
+DevModel model_from(int norb, int nbath, const double* em, const double* ek, const double* vmk, double U,
+                    double Up, double Jex, double Jp, double mu)
+{
+    arg_check(norb >= 1 && norb <= EDZT_MAX_NORB, "norb must be in [1, 4]");
+    arg_check(nbath >= 0 && norb + nbath <= EDZT_MAX_NSITE, "norb + nbath must be <= 20");
+    arg_check(em != nullptr && (nbath == 0 || (ek != nullptr && vmk != nullptr)), "em/ek/vmk required");
+    DevModel m{};
+    m.norb = norb; m.nbath = nbath; m.nsite = norb + nbath;
+    for (int s = 0; s < 2; s++) {
+        for (int a = 0; a < norb; a++) m.em[a][s] = em[a + norb * s];
+        for (int l = 0; l < nbath; l++) m.ek[l][s] = ek[l + nbath * s];
+        for (int a = 0; a < norb; a++)
+            for (int l = 0; l < nbath; l++) m.vmk[a][l][s] = vmk[a + norb * (l + nbath * s)];
+    }
+    m.U = U; m.Up = Up; m.Jex = Jex; m.Jp = Jp; m.mu = mu;
+    return m;
+}
+
+void set_tables_model(ModelTables& mt, const DevModel& m, cudaStream_t stream)
+{
+    mt.ops.clear();
+    mt.model = m;
+    build_model_tables(mt, stream);
+    mt.valid = true;
 }
 
 // ---------------------------------------------------------------------------
@@ -415,6 +445,7 @@ void copy_out(edzt_ctx* c, void* dst, const void* src, size_t bytes)
 // batched persistent Lanczos
 // ---------------------------------------------------------------------------
 struct JobSpec {
+    ModelTables* mt = nullptr;       // model of the run (nullptr: the context's)
     int nu = 0, nd = 0;
     int mode = LZ_COEFF;
     int init = LZ_INIT_HASH;
@@ -454,7 +485,7 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
         JobSpec& s = specs[j];
         LzJob& J = jobs[j];
         std::memset(&J, 0, sizeof(J));
-        J.S = make_sector(c, s.nu, s.nd);
+        J.S = make_sector_mt(c, s.mt ? *s.mt : c->mt, s.nu, s.nd);
         const long long dim = J.S.dim;
         for (int q = 0; q < 2; q++) {
             bufs.emplace_back(c->pool, (size_t)dim);
@@ -630,7 +661,7 @@ int plain_lanczos(edzt_ctx* c, const DevSector& S, const double* v_init, int max
 // ---------------------------------------------------------------------------
 void require_model(edzt_ctx* c)
 {
-    if (!c->has_model) throw EdztError{EDZT_ERR_STATE, "no model: call edzt_set_model first"};
+    if (!c->mt.valid) throw EdztError{EDZT_ERR_STATE, "no model: call edzt_set_model first"};
 }
 
 void check_sector(edzt_ctx* c, int nu, int nd)
@@ -786,6 +817,10 @@ void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnste
 
 // One c^+ or c run of green_diag.
 struct GreenRun {
+    ModelTables* mt = nullptr;     // model (nullptr: the context's, with its resident ground state)
+    const double* gs = nullptr;    // ground state of the run's model (device), sector (gs_up, gs_dn)
+    int gs_up = 0, gs_dn = 0;
+    double e0 = 0.0;
     int iorb, ispin, pm;
     int nu, nd;            // excitation sector
     int nstep = 0;
@@ -794,15 +829,16 @@ struct GreenRun {
     double* b = nullptr;
 };
 
-ApplyCArgs applyc_args(edzt_ctx* c, int in_up, int in_dn, int pm, int iorb, int ispin, int out_up, int out_dn)
+ApplyCArgs applyc_args_ns(edzt_ctx* c, int ns, int in_up, int in_dn, int pm, int iorb, int ispin, int out_up,
+                          int out_dn)
 {
     ApplyCArgs A{};
     A.pm = pm; A.iorb = iorb; A.ispin = ispin;
-    A.nsite = nsite_of(c);
-    StrTable& ou = str_table(c, out_up);
-    StrTable& od = str_table(c, out_dn);
-    StrTable& iu = str_table(c, in_up);
-    StrTable& idn = str_table(c, in_dn);
+    A.nsite = ns;
+    StrTable& ou = str_table_ns(c, ns, out_up);
+    StrTable& od = str_table_ns(c, ns, out_dn);
+    StrTable& iu = str_table_ns(c, ns, in_up);
+    StrTable& idn = str_table_ns(c, ns, in_dn);
     A.out_nup = ou.count; A.out_ndn = od.count;
     A.out_up_str = ou.str->as<uint32_t>();
     A.out_dn_str = od.str->as<uint32_t>();
@@ -810,6 +846,11 @@ ApplyCArgs applyc_args(edzt_ctx* c, int in_up, int in_dn, int pm, int iorb, int 
     A.in_up_rank = iu.rank->as<int32_t>();
     A.in_dn_rank = idn.rank->as<int32_t>();
     return A;
+}
+
+ApplyCArgs applyc_args(edzt_ctx* c, int in_up, int in_dn, int pm, int iorb, int ispin, int out_up, int out_dn)
+{
+    return applyc_args_ns(c, nsite_of(c), in_up, in_dn, pm, iorb, ispin, out_up, out_dn);
 }
 
 void excitation(int nu, int nd, int pm, int ispin, int* ou, int* od)
@@ -831,18 +872,22 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
         runs[r].a = ab.p + (size_t)(2 * r) * maxnstep;
         runs[r].b = ab.p + (size_t)(2 * r + 1) * maxnstep;
     }
+    for (GreenRun& g : runs)        // runs without a source use the context's resident ground state
+        if (!g.mt) { g.mt = &c->mt; g.gs = c->gs_vec.p; g.gs_up = c->gs_up; g.gs_dn = c->gs_dn; g.e0 = c->gs_e0; }
     std::vector<int> live;
     if (c->engine == EDZT_ENGINE_FUSED) {
         std::vector<JobSpec> specs;
         for (int r = 0; r < nr; r++) {
             GreenRun& g = runs[r];
-            if (sector_dim(c, g.nu, g.nd) <= 0) continue;
+            const int ns = g.mt->model.nsite;
+            if (sector_dim_ns(ns, g.nu, g.nd) <= 0) continue;
             JobSpec s;
+            s.mt = g.mt;
             s.nu = g.nu; s.nd = g.nd;
             s.mode = LZ_COEFF;
             s.init = LZ_INIT_APPLYC;
-            s.ac = applyc_args(c, c->gs_up, c->gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
-            s.ac_src = c->gs_vec.p;
+            s.ac = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
+            s.ac_src = g.gs;
             s.maxnstep = maxnstep;
             s.a = g.a; s.b = g.b;
             specs.push_back(s);
@@ -856,11 +901,12 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
     } else {
         for (int r = 0; r < nr; r++) {
             GreenRun& g = runs[r];
-            if (sector_dim(c, g.nu, g.nd) <= 0) continue;
-            DevSector S = make_sector(c, g.nu, g.nd);
+            const int ns = g.mt->model.nsite;
+            if (sector_dim_ns(ns, g.nu, g.nd) <= 0) continue;
+            DevSector S = make_sector_mt(c, *g.mt, g.nu, g.nd);
             Lease<double> vin(c->pool, (size_t)S.dim);
-            ApplyCArgs A = applyc_args(c, c->gs_up, c->gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
-            launch_apply_c(A, c->gs_vec.p, vin.p, c->stream);
+            ApplyCArgs A = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
+            launch_apply_c(A, g.gs, vin.p, c->stream);
             g_launches += 1;
             std::vector<double> ha(maxnstep), hb(maxnstep);
             g.nstep = plain_lanczos(c, S, vin.p, maxnstep, ha.data(), hb.data(), &g.norm0, nullptr, nullptr);
@@ -876,12 +922,12 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
     for (int r = 0; r < nr; r++) {
         GreenRun& gr = runs[r];
         if (gr.nstep < 1) continue;
-        CK(cudaMemcpyAsync(gr.b, &gr.norm0, sizeof(double), cudaMemcpyHostToDevice, c->stream));
         CFJob J;
         J.a = gr.a; J.b = gr.b;
+        J.b1 = gr.norm0;
         // a breakdown after the first vector is evaluated with a zero second level
         J.levels = (gr.nstep == 1 && maxnstep >= 2) ? 2 : gr.nstep;
-        J.zr_shift = (gr.pm == 1) ? c->gs_e0 : -c->gs_e0;
+        J.zr_shift = (gr.pm == 1) ? gr.e0 : -gr.e0;
         J.sign = (gr.pm == 1) ? -1.0 : 1.0;
         J.g = g.p + (size_t)r * 2 * nw;
         cj.push_back(J);
@@ -903,6 +949,7 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
     for (int r = 0; r < nr; r++) {
         g_out[r].assign(hg.begin() + (size_t)r * 2 * nw, hg.begin() + (size_t)(r + 1) * 2 * nw);
         ab_out[r].assign(hab.begin() + (size_t)(2 * r) * maxnstep, hab.begin() + (size_t)(2 * r + 2) * maxnstep);
+        if (runs[r].nstep >= 1) ab_out[r][maxnstep] = runs[r].norm0;       // b(1) (:219, :249)
     }
 }
 
@@ -919,7 +966,7 @@ void cluster_green_impl(edzt_ctx* c, int nspin, int maxnstep, int nw, const doub
     require_gs(c);
     arg_check(nspin == 1 || nspin == 2, "nspin must be 1 or 2");
     arg_check(maxnstep >= 1 && nw >= 0, "maxnstep >= 1, nw >= 0");
-    const int norb = c->model.norb;
+    const int norb = c->mt.model.norb;
     const bool even = !(nspin == 2 || c->gs_up != c->gs_dn);                    // :76-80
     std::vector<GreenRun> runs;
     for (int iorb = 1; iorb <= norb; iorb++)
@@ -979,7 +1026,7 @@ void green_diag_impl(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, con
 {
     require_model(c);
     require_gs(c);
-    arg_check(iorb >= 1 && iorb <= c->model.norb && (ispin == 1 || ispin == 2), "bad iorb/ispin");
+    arg_check(iorb >= 1 && iorb <= c->mt.model.norb && (ispin == 1 || ispin == 2), "bad iorb/ispin");
     arg_check(maxnstep >= 1 && nw >= 0, "maxnstep >= 1, nw >= 0");
     std::vector<GreenRun> runs(2);
     for (int pm = 1; pm <= 2; pm++) {
@@ -1035,10 +1082,11 @@ void edzt_count_launches(long long n) { g_launches += n; }
 
 int edzt_ctx_ready_sector(edzt_ctx* c, int nu, int nd, DevSector* S, const char** why)
 {
-    if (!c->has_model) { *why = "no model: call edzt_set_model first"; return EDZT_ERR_STATE; }
+    if (!c->mt.valid) { *why = "no model: call edzt_set_model first"; return EDZT_ERR_STATE; }
     if (!sector_valid(c, nu, nd)) { *why = "electron counts outside [0, nsite]"; return EDZT_ERR_ARG; }
-    const bool ready = c->str_tables.count(nu) && c->str_tables.count(nd) &&
-                       c->ops_tables.count(std::make_pair(nu, 0)) && c->ops_tables.count(std::make_pair(nd, 1));
+    const int ns = nsite_of(c);
+    const bool ready = c->str_tables.count(std::make_pair(ns, nu)) && c->str_tables.count(std::make_pair(ns, nd)) &&
+                       c->mt.ops.count(std::make_pair(nu, 0)) && c->mt.ops.count(std::make_pair(nd, 1));
     if (!ready) {
         *why = "the sector's tables are not built on this context: make one allocating call on the sector "
                "first (edzt_hx or edzt_lanczos_iteration)";
@@ -1157,31 +1205,15 @@ int edzt_set_model(edzt_ctx* c, int norb, int nbath, const double* em, const dou
                    double U, double Up, double Jex, double Jp, double mu)
 {
     return guarded(c, [&] {
-        arg_check(norb >= 1 && norb <= EDZT_MAX_NORB, "norb must be in [1, 4]");
-        arg_check(nbath >= 0 && norb + nbath <= EDZT_MAX_NSITE, "norb + nbath must be <= 20");
-        arg_check(em != nullptr && (nbath == 0 || (ek != nullptr && vmk != nullptr)), "em/ek/vmk required");
-        DevModel m{};
-        m.norb = norb; m.nbath = nbath; m.nsite = norb + nbath;
-        for (int s = 0; s < 2; s++) {
-            for (int a = 0; a < norb; a++) m.em[a][s] = em[a + norb * s];
-            for (int l = 0; l < nbath; l++) m.ek[l][s] = ek[l + nbath * s];
-            for (int a = 0; a < norb; a++)
-                for (int l = 0; l < nbath; l++) m.vmk[a][l][s] = vmk[a + norb * (l + nbath * s)];
-        }
-        m.U = U; m.Up = Up; m.Jex = Jex; m.Jp = Jp; m.mu = mu;
-        const bool same_nsite = c->has_model && c->model.nsite == m.nsite;
-        if (!same_nsite) c->str_tables.clear();
-        c->ops_tables.clear();
-        c->model = m;
-        c->has_model = true;
+        const DevModel m = model_from(norb, nbath, em, ek, vmk, U, Up, Jex, Jp, mu);
         c->has_gs = false;
-        build_model_tables(c);
+        set_tables_model(c->mt, m, c->stream);
     });
 }
 
 long long edzt_sector_dim(edzt_ctx* c, int ne_up, int ne_dn)
 {
-    if (!c || !c->has_model) return 0;
+    if (!c || !c->mt.valid) return 0;
     return sector_dim(c, ne_up, ne_dn);
 }
 
@@ -1204,9 +1236,9 @@ int edzt_basis_rank(edzt_ctx* c, int ne, int32_t* rank)
 {
     return guarded(c, [&] {
         require_model(c);
-        arg_check(ne >= 0 && ne <= c->model.nsite && rank != nullptr, "bad electron count or null rank");
+        arg_check(ne >= 0 && ne <= c->mt.model.nsite && rank != nullptr, "bad electron count or null rank");
         StrTable& s = str_table(c, ne);
-        copy_out(c, rank, s.rank->p, sizeof(int32_t) * ((size_t)1 << c->model.nsite));
+        copy_out(c, rank, s.rank->p, sizeof(int32_t) * ((size_t)1 << c->mt.model.nsite));
         CK(cudaStreamSynchronize(c->stream));
     });
 }
@@ -1235,7 +1267,7 @@ int edzt_apply_c(edzt_ctx* c, int ne_up, int ne_dn, const double* vec, int pm, i
         require_model(c);
         check_sector(c, ne_up, ne_dn);
         arg_check(pm == 1 || pm == 2, "pm must be 1 or 2");
-        arg_check(iorb >= 1 && iorb <= c->model.norb && (ispin == 1 || ispin == 2), "bad iorb/ispin");
+        arg_check(iorb >= 1 && iorb <= c->mt.model.norb && (ispin == 1 || ispin == 2), "bad iorb/ispin");
         arg_check(vec != nullptr && vec_out != nullptr, "vec and vec_out required");
         int ou, od;
         excitation(ne_up, ne_dn, pm, ispin, &ou, &od);

@@ -22,10 +22,11 @@ uint64_t edzt_binom(int n, int k);
 // Fills str[C(nsite,n)] (ascending) and rank[2^nsite] on the device.
 void launch_build_strings(int nsite, int n, uint32_t* str, int32_t* rank, cudaStream_t s);
 // Per-string tables of one spin species (sigma = 0 up, 1 down) for a model.
-// hpk: [hw/4][count] uint4 (packed hop entries, see edzt_hop_pack).
+// hpk: [hw/4][count] uint4 (packed hop entries, see edzt_hop_pack); amp:
+// [2*norb*nbath] (at least 2) amplitude slots.
 void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32_t* str, const int32_t* rank,
-                           int hw, double* e1, uint8_t* hcnt, uint32_t* hpk, uint8_t* imp, int32_t* sub,
-                           cudaStream_t s);
+                           int hw, double* e1, uint8_t* hcnt, uint32_t* hpk, double* amp, uint8_t* imp,
+                           int32_t* sub, cudaStream_t s);
 // Largest number of allowed hops of any string with n electrons of spin sigma.
 int edzt_max_hops(const DevModel& m, int sigma, int n);
 
@@ -49,7 +50,8 @@ void launch_apply_c(const ApplyCArgs& A, const double* in, double* out, cudaStre
 // Continued fractions (src/numeric_utils.f90:11-44) for many runs at once.
 struct CFJob {
     const double* a;      // [levels]
-    const double* b;      // [levels], b[0] = ||c^(+)|gs>||
+    const double* b;      // [levels], b[0] unused
+    double b1;            // b(1) = ||c^(+)|gs>|| (dmft_green.f90:219,249)
     int levels;           // number of CF levels (0: contributes nothing)
     double zr_shift;      // real part of z: +E0 for c^+, -E0 for c
     double sign;          // -1: z - a (continued_fraction_p), +1: z + a (continued_fraction_m)

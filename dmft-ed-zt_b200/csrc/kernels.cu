@@ -234,11 +234,14 @@ __global__ void k_cf(const CFJob* __restrict__ jobs, int njobs, const double* __
     const int n = J.levels;
     if (n < 1) return;
     const double zr = J.zr_shift, zi = omega[iw];
+    auto bk = [&](int i) { return i == 0 ? J.b1 : J.b[i]; };   // b(1) = ||c^(+)|gs>|
+    // the reference's recursion literally (numeric_utils.f90:18-22 / :39-43),
+    // including its final level with b(1) when n == 1
     double xr, xi;
-    cdiv_real(J.b[n - 1] * J.b[n - 1], zr + J.sign * J.a[n - 1], zi, &xr, &xi);
+    cdiv_real(bk(n - 1) * bk(n - 1), zr + J.sign * J.a[n - 1], zi, &xr, &xi);
     for (int i = n - 1; i >= 2; i--)
-        cdiv_real(J.b[i - 1] * J.b[i - 1], zr + J.sign * J.a[i - 1] - xr, zi - xi, &xr, &xi);
-    cdiv_real(J.b[0] * J.b[0], zr + J.sign * J.a[0] - xr, zi - xi, &xr, &xi);
+        cdiv_real(bk(i - 1) * bk(i - 1), zr + J.sign * J.a[i - 1] - xr, zi - xi, &xr, &xi);
+    cdiv_real(J.b1 * J.b1, zr + J.sign * J.a[0] - xr, zi - xi, &xr, &xi);
     J.g[2 * iw] = xr;
     J.g[2 * iw + 1] = xi;
 }

@@ -95,9 +95,17 @@ __global__ void k_build_rank(int nsite, int n, int32_t* __restrict__ rank)
 __global__ void k_build_spin_ops(DevModel m, int sigma, int count, const uint32_t* __restrict__ str,
                                  const int32_t* __restrict__ rank, int hw, double* __restrict__ e1,
                                  uint8_t* __restrict__ hcnt, uint32_t* __restrict__ hpk,
-                                 uint8_t* __restrict__ imp, int32_t* __restrict__ sub)
+                                 double* __restrict__ amp, uint8_t* __restrict__ imp, int32_t* __restrict__ sub)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) {   // amplitude slots: +V at 2c, -V at 2c+1, c = iorb*nbath + jbath
+        for (int a = 0; a < m.norb; a++)
+            for (int l = 0; l < m.nbath; l++) {
+                amp[2 * (a * m.nbath + l)] = m.vmk[a][l][sigma];
+                amp[2 * (a * m.nbath + l) + 1] = -m.vmk[a][l][sigma];
+            }
+        if (m.nbath == 0) amp[0] = amp[1] = 0.0;
+    }
     if (t >= count) return;
     const uint32_t u = str[t];
     const int norb = m.norb, nbath = m.nbath;
@@ -154,11 +162,11 @@ void launch_build_strings(int nsite, int n, uint32_t* str, int32_t* rank, cudaSt
 }
 
 void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32_t* str, const int32_t* rank,
-                           int hw, double* e1, uint8_t* hcnt, uint32_t* hpk, uint8_t* imp, int32_t* sub,
-                           cudaStream_t s)
+                           int hw, double* e1, uint8_t* hcnt, uint32_t* hpk, double* amp, uint8_t* imp,
+                           int32_t* sub, cudaStream_t s)
 {
-    if (count <= 0) return;
-    k_build_spin_ops<<<(count + 127) / 128, 128, 0, s>>>(m, sigma, count, str, rank, hw, e1, hcnt, hpk, imp, sub);
+    const int n = count > 0 ? count : 1;   // the amplitude slots are written even for an empty table
+    k_build_spin_ops<<<(n + 127) / 128, 128, 0, s>>>(m, sigma, count, str, rank, hw, e1, hcnt, hpk, amp, imp, sub);
 }
 
 int edzt_max_hops(const DevModel& m, int sigma, int n)
