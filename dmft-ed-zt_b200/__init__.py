@@ -48,11 +48,20 @@ EXPORTS = (
     "edzt_set_engine", "edzt_basis", "edzt_basis_rank", "edzt_sector_dim", "edzt_hx", "edzt_apply_c",
     "edzt_lanczos_iteration", "edzt_diag_lanczos", "edzt_ground_state", "edzt_gs_dim",
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
-    "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc",
+    "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
 )
 # Limits of edzt_lanczos_iteration_noalloc (its static scratch array).
 NOALLOC_MAX_DIM = 262144
 NOALLOC_MAX_STEPS = 2048
+
+
+class Instance(C.Structure):
+    """edzt_instance of include/edzt.h: one impurity solve of a batch."""
+    _fields_ = [("norb", C.c_int), ("nbath", C.c_int),
+                ("em", C.c_void_p), ("ek", C.c_void_p), ("vmk", C.c_void_p),
+                ("U", C.c_double), ("Up", C.c_double), ("Jex", C.c_double), ("Jp", C.c_double),
+                ("mu", C.c_double), ("nsector", C.c_int), ("sectors", C.c_void_p), ("nspin", C.c_int),
+                ("seed", C.c_uint64)]
 
 
 class EDError(RuntimeError):
@@ -100,6 +109,7 @@ def load_library(path: str = LIB_PATH):
     L.edzt_apply_c.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_int, _vp]
     L.edzt_lanczos_iteration.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
     L.edzt_lanczos_iteration_noalloc.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
+    L.edzt_solve_batch.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_size_t]
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
     L.edzt_ground_state.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_uint64, _ip, _dp, _vp, _vp]
     L.edzt_gs_dim.argtypes = [_vp]
@@ -321,6 +331,37 @@ class Solver:
                                                    _ptr(coeffs)))
         Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, norb, nw)
         return dict(G_cl=Gc, coeffs=coeffs.reshape(norb, 2, 4, maxnstep))
+
+    def solve_batch(self, instances, maxnstep, omega, hbm_budget=0):
+        """Many independent solves in batched persistent launches
+        (edzt_solve_batch).  instances: dicts with model, sectors, nspin (1),
+        seed (0).  Returns isector, e0 ([n]) and the per-instance G_cl arrays,
+        shaped (nspin, norb, nw) like solve()."""
+        omega = _f64(omega)
+        nw = omega.size
+        n = len(instances)
+        keep = []
+        arr = (Instance * max(n, 1))()
+        for i, inst in enumerate(instances):
+            m = inst["model"]
+            em, ek, vmk = m.fortran_arrays()
+            sec = np.ascontiguousarray(np.asarray(inst["sectors"], dtype=np.int32).reshape(-1, 2))
+            keep += [em, ek, vmk, sec]
+            arr[i] = Instance(m.norb, m.nbath, em.ctypes.data, ek.ctypes.data, vmk.ctypes.data, m.U, m.Up, m.Jex,
+                              m.Jp, m.mu, len(sec), sec.ctypes.data, int(inst.get("nspin", 1)),
+                              int(inst.get("seed", 0)))
+        sizes = [2 * nw * inst["model"].norb * int(inst.get("nspin", 1)) for inst in instances]
+        G = np.zeros(max(sum(sizes), 1))
+        isec = np.zeros(max(n, 1), dtype=np.int32)
+        e0 = np.zeros(max(n, 1))
+        self._check(self._L.edzt_solve_batch(self._h, n, C.addressof(arr), maxnstep, nw, _ptr(omega), _ptr(isec),
+                                             _ptr(e0), _ptr(G), int(hbm_budget)))
+        out, off = [], 0
+        for inst, sz in zip(instances, sizes):
+            g = G[off:off + sz]
+            off += sz
+            out.append((g[0::2] + 1j * g[1::2]).reshape(int(inst.get("nspin", 1)), inst["model"].norb, nw))
+        return dict(isector=isec[:n], e0=e0[:n], G_cl=out)
 
     def solve(self, sectors, maxnstep, omega, nspin=1, seed=0):
         """ground_state + cluster_green_ftn in one call (src/dmft.f90:76-78)."""

@@ -15,6 +15,7 @@
 #include <vector>
 #include <atomic>
 #include <algorithm>
+#include <thread>
 #include <cuda_runtime.h>
 #include "../../include/edzt.h"
 #include "edzt_internal.h"
@@ -958,48 +959,48 @@ void require_gs(edzt_ctx* c)
     if (!c->has_gs) throw EdztError{EDZT_ERR_STATE, "no resident ground state: call edzt_ground_state first"};
 }
 
-// cluster_green_ftn (dmft_green.f90:47-126)
-void cluster_green_impl(edzt_ctx* c, int nspin, int maxnstep, int nw, const double* omega, double* G_cl,
-                        double* coeffs)
+// The c^+ / c runs of cluster_green_ftn (dmft_green.f90:71-100) for a ground
+// state in sector (gs_up, gs_dn): per orbital, spin up and (unless even) down.
+std::vector<GreenRun> cluster_runs(int norb, bool even, int gs_up, int gs_dn)
 {
-    require_model(c);
-    require_gs(c);
-    arg_check(nspin == 1 || nspin == 2, "nspin must be 1 or 2");
-    arg_check(maxnstep >= 1 && nw >= 0, "maxnstep >= 1, nw >= 0");
-    const int norb = c->mt.model.norb;
-    const bool even = !(nspin == 2 || c->gs_up != c->gs_dn);                    // :76-80
     std::vector<GreenRun> runs;
     for (int iorb = 1; iorb <= norb; iorb++)
         for (int ispin = 1; ispin <= (even ? 1 : 2); ispin++)
             for (int pm = 1; pm <= 2; pm++) {
                 GreenRun g;
                 g.iorb = iorb; g.ispin = ispin; g.pm = pm;
-                excitation(c->gs_up, c->gs_dn, pm, ispin, &g.nu, &g.nd);
+                excitation(gs_up, gs_dn, pm, ispin, &g.nu, &g.nd);
                 runs.push_back(g);
             }
-    InVec om(c, omega, nw);
-    std::vector<std::vector<double>> gs, abs_;
-    green_runs(c, runs, maxnstep, nw, om.d, gs, abs_);
-    std::vector<double> Gh((size_t)2 * nw * norb * nspin, 0.0);
-    std::vector<double> ch((size_t)norb * 2 * 4 * maxnstep, 0.0);
-    int r = 0;
+    return runs;
+}
+
+// G_cl(nw, norb, nspin) (complex interleaved) and, nullable, the coefficient
+// rows coeffs[norb][2][4][maxnstep] from the results of cluster_runs, which
+// start at index r0 of gs / abs_ (dmft_green.f90:102-118).
+void assemble_cluster(int norb, int nspin, bool even, int maxnstep, int nw,
+                      const std::vector<std::vector<double>>& gs, const std::vector<std::vector<double>>& abs_,
+                      size_t r0, double* Gh, double* ch)
+{
+    size_t r = r0;
     for (int iorb = 1; iorb <= norb; iorb++) {
         std::vector<double> g1(2 * nw, 0.0), g2(2 * nw, 0.0);
         for (int ispin = 1; ispin <= (even ? 1 : 2); ispin++) {
             std::vector<double>& gg = (ispin == 1) ? g1 : g2;
             for (int pm = 1; pm <= 2; pm++, r++) {
                 for (int q = 0; q < 2 * nw; q++) gg[q] += gs[r][q];
+                if (!ch) continue;
                 const double* a = abs_[r].data();
                 const double* b = abs_[r].data() + maxnstep;
-                double* dst = ch.data() + ((size_t)(iorb - 1) * 2 + (ispin - 1)) * 4 * maxnstep;
+                double* dst = ch + ((size_t)(iorb - 1) * 2 + (ispin - 1)) * 4 * maxnstep;
                 double* da = dst + (pm == 1 ? 0 : 2) * maxnstep;
                 double* db = dst + (pm == 1 ? 1 : 3) * maxnstep;
                 std::memcpy(da, a, sizeof(double) * maxnstep);
                 std::memcpy(db, b, sizeof(double) * maxnstep);
             }
         }
-        if (even) {   // spin-down rows repeat spin-up (:102-109)
-            double* s1 = ch.data() + ((size_t)(iorb - 1) * 2) * 4 * maxnstep;
+        if (even && ch) {   // spin-down rows repeat spin-up (:102-109)
+            double* s1 = ch + ((size_t)(iorb - 1) * 2) * 4 * maxnstep;
             std::memcpy(s1 + 4 * maxnstep, s1, sizeof(double) * 4 * maxnstep);
         }
         for (int iw = 0; iw < nw; iw++) {                                       // :111-118
@@ -1016,6 +1017,25 @@ void cluster_green_impl(edzt_ctx* c, int nspin, int maxnstep, int nw, const doub
             }
         }
     }
+}
+
+// cluster_green_ftn (dmft_green.f90:47-126)
+void cluster_green_impl(edzt_ctx* c, int nspin, int maxnstep, int nw, const double* omega, double* G_cl,
+                        double* coeffs)
+{
+    require_model(c);
+    require_gs(c);
+    arg_check(nspin == 1 || nspin == 2, "nspin must be 1 or 2");
+    arg_check(maxnstep >= 1 && nw >= 0, "maxnstep >= 1, nw >= 0");
+    const int norb = c->mt.model.norb;
+    const bool even = !(nspin == 2 || c->gs_up != c->gs_dn);                    // :76-80
+    std::vector<GreenRun> runs = cluster_runs(norb, even, c->gs_up, c->gs_dn);
+    InVec om(c, omega, nw);
+    std::vector<std::vector<double>> gs, abs_;
+    green_runs(c, runs, maxnstep, nw, om.d, gs, abs_);
+    std::vector<double> Gh((size_t)2 * nw * norb * nspin, 0.0);
+    std::vector<double> ch((size_t)norb * 2 * 4 * maxnstep, 0.0);
+    assemble_cluster(norb, nspin, even, maxnstep, nw, gs, abs_, 0, Gh.data(), ch.data());
     if (G_cl) copy_out(c, G_cl, Gh.data(), sizeof(double) * Gh.size());
     if (coeffs) copy_out(c, coeffs, ch.data(), sizeof(double) * ch.size());
     CK(cudaStreamSynchronize(c->stream));
@@ -1045,6 +1065,207 @@ void green_diag_impl(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, con
     copy_out(c, am, abs_[1].data(), sizeof(double) * maxnstep);
     copy_out(c, bm, abs_[1].data() + maxnstep, sizeof(double) * maxnstep);
     copy_out(c, g, gsum.data(), sizeof(double) * 2 * nw);
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+// ---------------------------------------------------------------------------
+// batched solves: many independent impurity instances (each the
+// ground_state + cluster_green_ftn pair of src/dmft.f90:76-78), every phase
+// of all instances of a wave in one persistent launch
+// ---------------------------------------------------------------------------
+struct BatchInst {
+    DevModel model{};
+    std::vector<int> sec;          // [nsector][2]
+    int nspin = 1;
+    uint64_t seed = 0;
+    long long footprint = 0;       // device bytes the instance holds at its peak
+    std::unique_ptr<ModelTables> mt;
+    int best = -1, gs_up = 0, gs_dn = 0;
+    double e0 = 0.0;
+    Lease<double> gsvec;
+};
+
+template <class F>
+void parallel_for(int n, F&& f)
+{
+    const int nt = std::max(1, std::min(n, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next{0};
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; t++)
+        th.emplace_back([&] {
+            for (int i = next++; i < n; i = next++) f(i);
+        });
+    for (auto& x : th) x.join();
+}
+
+void solve_wave(edzt_ctx* c, std::vector<BatchInst>& B, int i0, int i1, int maxnstep, int nw,
+                const double* omega_dev, std::vector<double>& Gall, const std::vector<size_t>& goff)
+{
+    for (int i = i0; i < i1; i++) {
+        B[i].mt = std::make_unique<ModelTables>();
+        set_tables_model(*B[i].mt, B[i].model, c->stream);
+    }
+    // ---- ground-state scan: every sector of every instance (ground_state.f90:28-73)
+    struct Owner { int inst, sector; };
+    std::vector<JobSpec> specs;
+    std::vector<Owner> own;
+    for (int i = i0; i < i1; i++) {
+        const int ns = B[i].model.nsite;
+        for (size_t s = 0; s < B[i].sec.size() / 2; s++) {
+            const int nu = B[i].sec[2 * s], nd = B[i].sec[2 * s + 1];
+            if (sector_dim_ns(ns, nu, nd) <= 0) continue;
+            JobSpec j;
+            j.mt = B[i].mt.get();
+            j.nu = nu; j.nd = nd;
+            j.mode = LZ_COEFF;
+            j.init = LZ_INIT_HASH;
+            j.key = edzt_stream_key(B[i].seed, (uint64_t)s);
+            j.maxnstep = maxnstep;
+            specs.push_back(j);
+            own.push_back({i, (int)s});
+        }
+    }
+    const int nj = (int)specs.size();
+    Lease<double> ab(c->pool, (size_t)std::max(nj, 1) * 2 * maxnstep);
+    for (int q = 0; q < nj; q++) {
+        specs[q].a = ab.p + (size_t)(2 * q) * maxnstep;
+        specs[q].b = ab.p + (size_t)(2 * q + 1) * maxnstep;
+    }
+    run_jobs(c, specs);
+    std::vector<double> hab((size_t)std::max(nj, 1) * 2 * maxnstep);
+    CK(cudaMemcpyAsync(hab.data(), ab.p, sizeof(double) * hab.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<SectorResult> res(nj);
+    parallel_for(nj, [&](int q) {
+        SectorResult& r = res[q];
+        r.nstep = specs[q].nstep;
+        if (r.nstep < 1) return;
+        r.coeff.resize(r.nstep);
+        r.ok = edzt::lowest_eigenpair(r.nstep, hab.data() + (size_t)(2 * q) * maxnstep,
+                                      hab.data() + (size_t)(2 * q + 1) * maxnstep, &r.e, r.coeff.data()) == 0;
+    });
+    // selection per instance in sector order, 1e-10 relative tie band (ground_state.f90:62-68)
+    std::vector<int> win(B.size(), -1);
+    for (int q = 0; q < nj; q++) {
+        if (!res[q].ok) continue;
+        const int i = own[q].inst;
+        const int w = win[i];
+        const double tie = 1.0e-10 * std::max(1.0, std::fabs(w < 0 ? 0.0 : res[w].e));
+        if (w < 0 || res[q].e < res[w].e - tie) win[i] = q;
+    }
+    // ---- eigenvector pass of every winner (lanczos_solver.f90:213-300)
+    std::vector<JobSpec> ev;
+    Lease<double> coeffs(c->pool, (size_t)std::max(i1 - i0, 1) * maxnstep);
+    std::vector<double> hcoef((size_t)std::max(i1 - i0, 1) * maxnstep, 0.0);
+    for (int i = i0; i < i1; i++) {
+        const int q = win[i];
+        if (q < 0) throw EdztError{EDZT_ERR_NUMERIC, "instance " + std::to_string(i) + ": no sector produced a ground state"};
+        BatchInst& I = B[i];
+        I.best = own[q].sector;
+        I.gs_up = specs[q].nu; I.gs_dn = specs[q].nd;
+        I.e0 = res[q].e;
+        I.gsvec = Lease<double>(c->pool, (size_t)sector_dim_ns(I.model.nsite, I.gs_up, I.gs_dn));
+        std::copy(res[q].coeff.begin(), res[q].coeff.end(), hcoef.begin() + (size_t)(i - i0) * maxnstep);
+        JobSpec j;
+        j.mt = I.mt.get();
+        j.nu = I.gs_up; j.nd = I.gs_dn;
+        j.mode = LZ_EIGVEC;
+        j.init = LZ_INIT_HASH;
+        j.key = specs[q].key;
+        j.maxnstep = res[q].nstep;
+        j.coeff = coeffs.p + (size_t)(i - i0) * maxnstep;
+        j.eig = I.gsvec.p;
+        j.a = specs[q].a;            // the coefficients of the scan, still on the device
+        j.b = specs[q].b;
+        ev.push_back(j);
+    }
+    CK(cudaMemcpyAsync(coeffs.p, hcoef.data(), sizeof(double) * hcoef.size(), cudaMemcpyHostToDevice, c->stream));
+    run_jobs(c, ev);
+    for (int i = i0; i < i1; i++) {   // normalise (lanczos_solver.f90:291)
+        const long long n = sector_dim_ns(B[i].model.nsite, B[i].gs_up, B[i].gs_dn);
+        launch_dot(B[i].gsvec.p, B[i].gsvec.p, n, c->dot_part->as<double>(), c->scal->as<double>(), c->stream);
+        launch_scale_inv_sqrt(B[i].gsvec.p, n, c->scal->as<double>(), c->stream);
+        g_launches += 3;
+    }
+    CKLAUNCH();
+    // ---- Green's function runs of every instance (dmft_green.f90:47-126)
+    std::vector<GreenRun> runs;
+    std::vector<size_t> r0(B.size(), 0);
+    for (int i = i0; i < i1; i++) {
+        BatchInst& I = B[i];
+        const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
+        r0[i] = runs.size();
+        for (GreenRun g : cluster_runs(I.model.norb, even, I.gs_up, I.gs_dn)) {
+            g.mt = I.mt.get();
+            g.gs = I.gsvec.p;
+            g.gs_up = I.gs_up; g.gs_dn = I.gs_dn;
+            g.e0 = I.e0;
+            runs.push_back(g);
+        }
+    }
+    std::vector<std::vector<double>> gs, abs_;
+    green_runs(c, runs, maxnstep, nw, omega_dev, gs, abs_);
+    for (int i = i0; i < i1; i++) {
+        BatchInst& I = B[i];
+        const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
+        assemble_cluster(I.model.norb, I.nspin, even, maxnstep, nw, gs, abs_, r0[i], Gall.data() + goff[i], nullptr);
+        I.gsvec.reset();
+        I.mt.reset();
+    }
+}
+
+void solve_batch_impl(edzt_ctx* c, int ninst, const edzt_instance* inst, int maxnstep, int nw, const double* omega,
+                      int* isector, double* e0, double* G_cl, size_t budget)
+{
+    arg_check(ninst >= 0 && (ninst == 0 || inst != nullptr), "ninst >= 0 and inst required");
+    arg_check(maxnstep >= 1 && nw >= 0 && (nw == 0 || omega != nullptr), "maxnstep >= 1, nw >= 0, omega");
+    std::vector<BatchInst> B(ninst);
+    std::vector<size_t> goff(ninst + 1, 0);
+    for (int i = 0; i < ninst; i++) {
+        const edzt_instance& in = inst[i];
+        BatchInst& I = B[i];
+        I.model = model_from(in.norb, in.nbath, in.em, in.ek, in.vmk, in.U, in.Up, in.Jex, in.Jp, in.mu);
+        arg_check(in.nsector >= 1 && in.sectors != nullptr, "every instance needs nsector >= 1 sectors");
+        arg_check(in.nspin == 1 || in.nspin == 2, "nspin must be 1 or 2");
+        I.sec.assign(in.sectors, in.sectors + 2 * in.nsector);
+        I.nspin = in.nspin;
+        I.seed = in.seed;
+        const int ns = I.model.nsite;
+        long long gsb = 0, maxd = 0, maxe = 0;
+        for (int s = 0; s < in.nsector; s++) {
+            const int nu = I.sec[2 * s], nd = I.sec[2 * s + 1];
+            arg_check(sector_valid_ns(ns, nu, nd), "electron counts outside [0, nsite]");
+            const long long d = sector_dim_ns(ns, nu, nd);
+            gsb += 32 * d;
+            maxd = std::max(maxd, d);
+            for (int du = -1; du <= 1; du++)
+                for (int dd = -1; dd <= 1; dd++)
+                    if ((du == 0) != (dd == 0)) maxe = std::max(maxe, sector_dim_ns(ns, nu + du, nd + dd));
+        }
+        const long long cfb = 4LL * I.model.norb * 32 * maxe + 8 * maxd;
+        I.footprint = std::max(gsb, cfb) + 48 * maxd;
+        goff[i + 1] = goff[i] + (size_t)2 * nw * I.model.norb * I.nspin;
+    }
+    if (budget == 0) {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        budget = fr / 10 * 8;
+    }
+    InVec om(c, omega, nw);
+    std::vector<double> Gall(std::max(goff[ninst], (size_t)1), 0.0);
+    for (int i0 = 0; i0 < ninst;) {   // waves that fit the device-memory budget
+        int i1 = i0;
+        long long sum = 0;
+        while (i1 < ninst && (i1 == i0 || sum + B[i1].footprint <= (long long)budget)) sum += B[i1++].footprint;
+        solve_wave(c, B, i0, i1, maxnstep, nw, om.d, Gall, goff);
+        c->pool.trim();
+        i0 = i1;
+    }
+    for (int i = 0; i < ninst; i++) {
+        if (isector) isector[i] = B[i].best;
+        if (e0) e0[i] = B[i].e0;
+    }
+    if (G_cl && goff[ninst] > 0) copy_out(c, G_cl, Gall.data(), sizeof(double) * goff[ninst]);
     CK(cudaStreamSynchronize(c->stream));
 }
 
@@ -1371,6 +1592,12 @@ int edzt_cluster_green_ftn(edzt_ctx* c, int nspin, int maxnstep, int nw, const d
         arg_check(G_cl != nullptr && (omega || nw == 0), "bad arguments");
         cluster_green_impl(c, nspin, maxnstep, nw, omega, G_cl, coeffs);
     });
+}
+
+int edzt_solve_batch(edzt_ctx* c, int ninst, const edzt_instance* inst, int maxnstep, int nw, const double* omega,
+                     int* isector, double* e0, double* G_cl, size_t hbm_budget)
+{
+    return guarded(c, [&] { solve_batch_impl(c, ninst, inst, maxnstep, nw, omega, isector, e0, G_cl, hbm_budget); });
 }
 
 int edzt_solve(edzt_ctx* c, int nsector, const int* sectors, int maxnstep, uint64_t seed, int nspin, int nw,

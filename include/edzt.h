@@ -156,9 +156,34 @@ int edzt_cluster_green_ftn(edzt_ctx *ctx, int nspin, int maxnstep, int nw, const
                            double *G_cl, double *coeffs);
 
 /* One impurity solve: edzt_ground_state followed by edzt_cluster_green_ftn
- * (the calls at src/dmft.f90:76-78).  gsvec, e_sector, coeffs nullable. */
+ * (the calls at src/dmft.f90:76-78).  G_cl and coeffs nullable. */
 int edzt_solve(edzt_ctx *ctx, int nsector, const int *sectors, int maxnstep, uint64_t seed, int nspin,
                int nw, const double *omega, int *isector, double *e0, double *G_cl, double *coeffs);
+
+/* One impurity instance of a batch: the arguments of edzt_set_model, of
+ * edzt_ground_state and of edzt_cluster_green_ftn for one solve.  Arrays are
+ * host memory in the layouts above; sectors is [nsector][2] (ne_up, ne_dn);
+ * sector i starts Lanczos from stream i of seed. */
+typedef struct edzt_instance {
+    int norb, nbath;
+    const double *em, *ek, *vmk;
+    double U, Up, Jex, Jp, mu;
+    int nsector;
+    const int *sectors;
+    int nspin;
+    uint64_t seed;
+} edzt_instance;
+
+/* Batched form of edzt_solve (the ground_state + cluster_green_ftn pair of
+ * src/dmft.f90:76-78) for ninst independent instances of uneven Fock
+ * dimension: the sector scans of all instances run in one persistent launch,
+ * then all eigenvector passes, then all c / c^+ runs, in waves whose device
+ * memory stays within hbm_budget bytes (0: 80% of the free memory).  Each
+ * instance's results are those of edzt_solve on it alone, to rounding.
+ * isector, e0: [ninst] (nullable); G_cl (nullable, host or device): the
+ * instances' G_cl(nw, norb, nspin) complex arrays, concatenated in order. */
+int edzt_solve_batch(edzt_ctx *ctx, int ninst, const edzt_instance *inst, int maxnstep, int nw,
+                     const double *omega, int *isector, double *e0, double *G_cl, size_t hbm_budget);
 
 /* Kernel launches issued by this context since creation (instrumentation). */
 long long edzt_launch_count(const edzt_ctx *ctx);
