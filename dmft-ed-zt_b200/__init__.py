@@ -49,6 +49,7 @@ EXPORTS = (
     "edzt_lanczos_iteration", "edzt_diag_lanczos", "edzt_ground_state", "edzt_gs_dim",
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
     "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
+    "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
 )
 # Limits of edzt_lanczos_iteration_noalloc (its static scratch array).
 NOALLOC_MAX_DIM = 262144
@@ -62,6 +63,15 @@ class Instance(C.Structure):
                 ("U", C.c_double), ("Up", C.c_double), ("Jex", C.c_double), ("Jp", C.c_double),
                 ("mu", C.c_double), ("nsector", C.c_int), ("sectors", C.c_void_p), ("nspin", C.c_int),
                 ("seed", C.c_uint64)]
+
+
+def _instance(inst, keep):
+    m = inst["model"]
+    em, ek, vmk = m.fortran_arrays()
+    sec = np.ascontiguousarray(np.asarray(inst["sectors"], dtype=np.int32).reshape(-1, 2))
+    keep += [em, ek, vmk, sec]
+    return Instance(m.norb, m.nbath, em.ctypes.data, ek.ctypes.data, vmk.ctypes.data, m.U, m.Up, m.Jex, m.Jp, m.mu,
+                    len(sec), sec.ctypes.data, int(inst.get("nspin", 1)), int(inst.get("seed", 0)))
 
 
 class EDError(RuntimeError):
@@ -110,6 +120,12 @@ def load_library(path: str = LIB_PATH):
     L.edzt_lanczos_iteration.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
     L.edzt_lanczos_iteration_noalloc.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
     L.edzt_solve_batch.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_size_t]
+    L.edzt_server_create.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_size_t, C.POINTER(C.c_void_p)]
+    L.edzt_server_submit.argtypes = [_vp, _vp, C.POINTER(C.c_longlong)]
+    L.edzt_server_step.argtypes = [_vp, _ip, _ip, _ip]
+    L.edzt_server_result.argtypes = [_vp, C.c_longlong, _ip, _ip, _dp, _vp]
+    L.edzt_server_destroy.argtypes = [_vp]
+    L.edzt_server_destroy.restype = None
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
     L.edzt_ground_state.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_uint64, _ip, _dp, _vp, _vp]
     L.edzt_gs_dim.argtypes = [_vp]
@@ -343,13 +359,7 @@ class Solver:
         keep = []
         arr = (Instance * max(n, 1))()
         for i, inst in enumerate(instances):
-            m = inst["model"]
-            em, ek, vmk = m.fortran_arrays()
-            sec = np.ascontiguousarray(np.asarray(inst["sectors"], dtype=np.int32).reshape(-1, 2))
-            keep += [em, ek, vmk, sec]
-            arr[i] = Instance(m.norb, m.nbath, em.ctypes.data, ek.ctypes.data, vmk.ctypes.data, m.U, m.Up, m.Jex,
-                              m.Jp, m.mu, len(sec), sec.ctypes.data, int(inst.get("nspin", 1)),
-                              int(inst.get("seed", 0)))
+            arr[i] = _instance(inst, keep)
         sizes = [2 * nw * inst["model"].norb * int(inst.get("nspin", 1)) for inst in instances]
         G = np.zeros(max(sum(sizes), 1))
         isec = np.zeros(max(n, 1), dtype=np.int32)
@@ -374,3 +384,93 @@ class Solver:
         self._check(self._L.edzt_solve(self._h, len(sec), _ptr(sec), maxnstep, C.c_uint64(seed), nspin, nw,
                                        _ptr(omega), C.byref(isec), C.byref(e0), _ptr(G), None))
         return dict(isector=isec.value, e0=e0.value, G_cl=(G[0::2] + 1j * G[1::2]).reshape(nspin, norb, nw))
+
+
+class Server:
+    """Served form (edzt_server_*): continuous batching of impurity solves on
+    one solver context.  submit() queues a request (a dict like solve_batch's
+    instances), step() admits what fits in device memory and advances every
+    admitted request by one phase in one persistent launch, result() returns
+    a finished request's isector, e0 and G_cl (nspin, norb, nw), else None."""
+
+    def __init__(self, solver: "Solver", maxnstep: int, omega, hbm_budget: int = 0):
+        self.solver = solver
+        self._L = solver._L
+        self.omega = _f64(omega)
+        self.nw = self.omega.size
+        self.maxnstep = maxnstep
+        h = C.c_void_p()
+        solver._check(self._L.edzt_server_create(solver._h, maxnstep, self.nw, _ptr(self.omega), int(hbm_budget),
+                                                 C.byref(h)))
+        self._h = h
+        self._shape = {}
+
+    def submit(self, inst) -> int:
+        keep = []
+        rec = _instance(inst, keep)
+        rid = C.c_longlong()
+        self.solver._check(self._L.edzt_server_submit(self._h, C.byref(rec), C.byref(rid)))
+        self._shape[rid.value] = (int(inst.get("nspin", 1)), inst["model"].norb)
+        return rid.value
+
+    def step(self):
+        na, nq, nf = C.c_int(), C.c_int(), C.c_int()
+        self.solver._check(self._L.edzt_server_step(self._h, C.byref(na), C.byref(nq), C.byref(nf)))
+        return na.value, nq.value, nf.value
+
+    def result(self, rid: int):
+        nspin, norb = self._shape[rid]
+        G = np.zeros(2 * self.nw * norb * nspin)
+        done, isec, e0 = C.c_int(), C.c_int(), C.c_double()
+        self.solver._check(self._L.edzt_server_result(self._h, rid, C.byref(done), C.byref(isec), C.byref(e0),
+                                                      _ptr(G)))
+        if not done.value:
+            return None
+        del self._shape[rid]
+        return dict(isector=isec.value, e0=e0.value, G_cl=(G[0::2] + 1j * G[1::2]).reshape(nspin, norb, self.nw))
+
+    def close(self):
+        if self._h:
+            self._L.edzt_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve(server: Server, requests, arrivals):
+    """Request loop of the served form: request i is submitted once the wall
+    clock passes arrivals[i] (seconds from the start); the server steps while
+    work is queued or running and idles until the next arrival otherwise.
+    Returns (results in request order, latency of each request in seconds
+    from its arrival to the end of the step that finished it, total seconds)."""
+    import time
+    order = np.argsort(np.asarray(arrivals, dtype=float), kind="stable")
+    ids = [None] * len(requests)
+    done = [None] * len(requests)
+    lat = np.zeros(len(requests))
+    t0 = time.perf_counter()
+    nxt = 0
+    pending = set()
+    while nxt < len(order) or pending:
+        now = time.perf_counter() - t0
+        while nxt < len(order) and arrivals[order[nxt]] <= now:
+            i = int(order[nxt])
+            ids[i] = server.submit(requests[i])
+            pending.add(i)
+            nxt += 1
+        if not pending:
+            time.sleep(max(0.0, arrivals[order[nxt]] - now))
+            continue
+        server.step()
+        t = time.perf_counter() - t0
+        for i in list(pending):
+            r = server.result(ids[i])
+            if r is not None:
+                done[i] = r
+                lat[i] = t - arrivals[i]
+                pending.discard(i)
+    return done, lat, time.perf_counter() - t0

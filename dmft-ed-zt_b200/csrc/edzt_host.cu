@@ -15,6 +15,7 @@
 #include <vector>
 #include <atomic>
 #include <algorithm>
+#include <deque>
 #include <thread>
 #include <cuda_runtime.h>
 #include "../../include/edzt.h"
@@ -1214,6 +1215,33 @@ void solve_wave(edzt_ctx* c, std::vector<BatchInst>& B, int i0, int i1, int maxn
     }
 }
 
+// Validate one instance and estimate the device memory it holds at its peak
+// (sector scan: 32 B per state of every sector; Green's runs: 4*norb runs of
+// the largest neighbouring sector plus the ground state).
+void init_inst(const edzt_instance& in, BatchInst& I)
+{
+    I.model = model_from(in.norb, in.nbath, in.em, in.ek, in.vmk, in.U, in.Up, in.Jex, in.Jp, in.mu);
+    arg_check(in.nsector >= 1 && in.sectors != nullptr, "every instance needs nsector >= 1 sectors");
+    arg_check(in.nspin == 1 || in.nspin == 2, "nspin must be 1 or 2");
+    I.sec.assign(in.sectors, in.sectors + 2 * in.nsector);
+    I.nspin = in.nspin;
+    I.seed = in.seed;
+    const int ns = I.model.nsite;
+    long long gsb = 0, maxd = 0, maxe = 0;
+    for (int s = 0; s < in.nsector; s++) {
+        const int nu = I.sec[2 * s], nd = I.sec[2 * s + 1];
+        arg_check(sector_valid_ns(ns, nu, nd), "electron counts outside [0, nsite]");
+        const long long d = sector_dim_ns(ns, nu, nd);
+        gsb += 32 * d;
+        maxd = std::max(maxd, d);
+        for (int du = -1; du <= 1; du++)
+            for (int dd = -1; dd <= 1; dd++)
+                if ((du == 0) != (dd == 0)) maxe = std::max(maxe, sector_dim_ns(ns, nu + du, nd + dd));
+    }
+    const long long cfb = 4LL * I.model.norb * 32 * maxe + 8 * maxd;
+    I.footprint = std::max(gsb, cfb) + 48 * maxd;
+}
+
 void solve_batch_impl(edzt_ctx* c, int ninst, const edzt_instance* inst, int maxnstep, int nw, const double* omega,
                       int* isector, double* e0, double* G_cl, size_t budget)
 {
@@ -1222,29 +1250,8 @@ void solve_batch_impl(edzt_ctx* c, int ninst, const edzt_instance* inst, int max
     std::vector<BatchInst> B(ninst);
     std::vector<size_t> goff(ninst + 1, 0);
     for (int i = 0; i < ninst; i++) {
-        const edzt_instance& in = inst[i];
-        BatchInst& I = B[i];
-        I.model = model_from(in.norb, in.nbath, in.em, in.ek, in.vmk, in.U, in.Up, in.Jex, in.Jp, in.mu);
-        arg_check(in.nsector >= 1 && in.sectors != nullptr, "every instance needs nsector >= 1 sectors");
-        arg_check(in.nspin == 1 || in.nspin == 2, "nspin must be 1 or 2");
-        I.sec.assign(in.sectors, in.sectors + 2 * in.nsector);
-        I.nspin = in.nspin;
-        I.seed = in.seed;
-        const int ns = I.model.nsite;
-        long long gsb = 0, maxd = 0, maxe = 0;
-        for (int s = 0; s < in.nsector; s++) {
-            const int nu = I.sec[2 * s], nd = I.sec[2 * s + 1];
-            arg_check(sector_valid_ns(ns, nu, nd), "electron counts outside [0, nsite]");
-            const long long d = sector_dim_ns(ns, nu, nd);
-            gsb += 32 * d;
-            maxd = std::max(maxd, d);
-            for (int du = -1; du <= 1; du++)
-                for (int dd = -1; dd <= 1; dd++)
-                    if ((du == 0) != (dd == 0)) maxe = std::max(maxe, sector_dim_ns(ns, nu + du, nd + dd));
-        }
-        const long long cfb = 4LL * I.model.norb * 32 * maxe + 8 * maxd;
-        I.footprint = std::max(gsb, cfb) + 48 * maxd;
-        goff[i + 1] = goff[i] + (size_t)2 * nw * I.model.norb * I.nspin;
+        init_inst(inst[i], B[i]);
+        goff[i + 1] = goff[i] + (size_t)2 * nw * B[i].model.norb * B[i].nspin;
     }
     if (budget == 0) {
         size_t fr = 0, tot = 0;
@@ -1267,6 +1274,257 @@ void solve_batch_impl(edzt_ctx* c, int ninst, const edzt_instance* inst, int max
     }
     if (G_cl && goff[ninst] > 0) copy_out(c, G_cl, Gall.data(), sizeof(double) * goff[ninst]);
     CK(cudaStreamSynchronize(c->stream));
+}
+
+// ---------------------------------------------------------------------------
+// served form: continuous batching of impurity solves.  A request advances
+// one phase per step (sector scan, eigenvector pass, c / c^+ runs with the
+// continued fractions); every step is one persistent launch that carries the
+// current phase of every active request, and requests queued meanwhile are
+// admitted at the next step when their device-memory footprint fits.
+// ---------------------------------------------------------------------------
+struct ServReq {
+    long long id = 0;
+    BatchInst I;
+    int phase = 0;                         // 1 scan, 2 eigenvector, 3 Green's runs, 4 done
+    Lease<double> ab;                      // [nsector][2][maxnstep] scan coefficients (device)
+    std::vector<int> job_of_sector;        // scan job of each sector in the current launch, -1 if none
+    std::vector<double> hab;               // scan coefficients on the host
+    std::vector<SectorResult> res;
+    int win = -1;                          // winning sector
+    Lease<double> coef;                    // tridiagonal eigenvector of the winner (device)
+    std::vector<GreenRun> runs;
+    Lease<double> gab;                     // [nruns][2][maxnstep] Green's-run coefficients (device)
+    std::vector<double> G;                 // G_cl(nw, norb, nspin), complex interleaved
+    std::string error;
+};
+
+}  // namespace
+
+struct edzt_server {
+    edzt_ctx* c = nullptr;
+    int maxnstep = 0, nw = 0;
+    std::unique_ptr<DevBuf> omega;
+    long long budget = 0, reserved = 0, next_id = 1;
+    std::deque<std::unique_ptr<ServReq>> queue;
+    std::vector<std::unique_ptr<ServReq>> active;
+    std::map<long long, std::unique_ptr<ServReq>> finished;
+};
+
+namespace {
+
+void server_admit(edzt_server* sv)
+{
+    edzt_ctx* c = sv->c;
+    while (!sv->queue.empty()) {
+        ServReq& q = *sv->queue.front();
+        if (!sv->active.empty() && sv->reserved + q.I.footprint > sv->budget) break;
+        sv->reserved += q.I.footprint;
+        q.I.mt = std::make_unique<ModelTables>();
+        set_tables_model(*q.I.mt, q.I.model, c->stream);
+        const int ns = (int)q.I.sec.size() / 2;
+        q.ab = Lease<double>(c->pool, (size_t)std::max(ns, 1) * 2 * sv->maxnstep);
+        q.phase = 1;
+        sv->active.push_back(std::move(sv->queue.front()));
+        sv->queue.pop_front();
+    }
+}
+
+// One step: the current phase of every active request in one launch.
+int server_step(edzt_server* sv)
+{
+    edzt_ctx* c = sv->c;
+    const int maxnstep = sv->maxnstep, nw = sv->nw;
+    server_admit(sv);
+    std::vector<JobSpec> specs;
+    for (auto& up : sv->active) {
+        ServReq& q = *up;
+        BatchInst& I = q.I;
+        const int ns = I.model.nsite;
+        if (q.phase == 1) {                                   // sector scan (ground_state.f90:28-73)
+            const int nsec = (int)I.sec.size() / 2;
+            q.job_of_sector.assign(nsec, -1);
+            for (int s = 0; s < nsec; s++) {
+                const int nu = I.sec[2 * s], nd = I.sec[2 * s + 1];
+                if (sector_dim_ns(ns, nu, nd) <= 0) continue;
+                JobSpec j;
+                j.mt = I.mt.get();
+                j.nu = nu; j.nd = nd;
+                j.mode = LZ_COEFF;
+                j.init = LZ_INIT_HASH;
+                j.key = edzt_stream_key(I.seed, (uint64_t)s);
+                j.maxnstep = maxnstep;
+                j.a = q.ab.p + (size_t)(2 * s) * maxnstep;
+                j.b = q.ab.p + (size_t)(2 * s + 1) * maxnstep;
+                q.job_of_sector[s] = (int)specs.size();
+                specs.push_back(j);
+            }
+        } else if (q.phase == 2) {                            // eigenvector pass (lanczos_solver.f90:213-300)
+            const SectorResult& r = q.res[q.win];
+            JobSpec j;
+            j.mt = I.mt.get();
+            j.nu = I.gs_up; j.nd = I.gs_dn;
+            j.mode = LZ_EIGVEC;
+            j.init = LZ_INIT_HASH;
+            j.key = edzt_stream_key(I.seed, (uint64_t)q.win);
+            j.maxnstep = r.nstep;
+            j.coeff = q.coef.p;
+            j.eig = I.gsvec.p;
+            j.a = q.ab.p + (size_t)(2 * q.win) * maxnstep;
+            j.b = q.ab.p + (size_t)(2 * q.win + 1) * maxnstep;
+            specs.push_back(j);
+        } else if (q.phase == 3) {                            // c / c^+ runs (dmft_green.f90:204-250)
+            for (size_t r = 0; r < q.runs.size(); r++) {
+                GreenRun& g = q.runs[r];
+                g.a = q.gab.p + (2 * r) * maxnstep;
+                g.b = q.gab.p + (2 * r + 1) * maxnstep;
+                g.nstep = 0;
+                if (sector_dim_ns(ns, g.nu, g.nd) <= 0) continue;
+                JobSpec j;
+                j.mt = I.mt.get();
+                j.nu = g.nu; j.nd = g.nd;
+                j.mode = LZ_COEFF;
+                j.init = LZ_INIT_APPLYC;
+                j.ac = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
+                j.ac_src = g.gs;
+                j.maxnstep = maxnstep;
+                j.a = g.a; j.b = g.b;
+                g.nstep = -1 - (int)specs.size();             // its job, resolved after the launch
+                specs.push_back(j);
+            }
+        }
+    }
+    if (specs.empty()) return 0;
+    run_jobs(c, specs);
+
+    // after the launch: every request moves one phase on
+    std::vector<ServReq*> scan, eig, green;
+    for (auto& up : sv->active) {
+        if (up->phase == 1) scan.push_back(up.get());
+        else if (up->phase == 2) eig.push_back(up.get());
+        else if (up->phase == 3) green.push_back(up.get());
+    }
+    for (ServReq* q : scan) {                                 // tridiagonal ground state per sector
+        const int nsec = (int)q->I.sec.size() / 2;
+        q->hab.assign((size_t)std::max(nsec, 1) * 2 * maxnstep, 0.0);
+        CK(cudaMemcpyAsync(q->hab.data(), q->ab.p, sizeof(double) * q->hab.size(), cudaMemcpyDeviceToHost,
+                           c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    for (ServReq* q : scan) {
+        const int nsec = (int)q->I.sec.size() / 2;
+        q->res.assign(nsec, SectorResult{});
+        parallel_for(nsec, [&](int s) {
+            const int jq = q->job_of_sector[s];
+            if (jq < 0) return;
+            SectorResult& r = q->res[s];
+            r.nstep = specs[jq].nstep;
+            if (r.nstep < 1) return;
+            r.coeff.resize(r.nstep);
+            r.ok = edzt::lowest_eigenpair(r.nstep, q->hab.data() + (size_t)(2 * s) * maxnstep,
+                                          q->hab.data() + (size_t)(2 * s + 1) * maxnstep, &r.e,
+                                          r.coeff.data()) == 0;
+        });
+        int w = -1;                                           // ground_state.f90:62-68, 1e-10 tie band
+        for (int s = 0; s < nsec; s++) {
+            if (!q->res[s].ok) continue;
+            const double tie = 1.0e-10 * std::max(1.0, std::fabs(w < 0 ? 0.0 : q->res[w].e));
+            if (w < 0 || q->res[s].e < q->res[w].e - tie) w = s;
+        }
+        if (w < 0) { q->error = "no sector produced a ground state"; q->phase = 4; continue; }
+        q->win = w;
+        q->I.best = w;
+        q->I.gs_up = q->I.sec[2 * w]; q->I.gs_dn = q->I.sec[2 * w + 1];
+        q->I.e0 = q->res[w].e;
+        q->I.gsvec = Lease<double>(c->pool, (size_t)sector_dim_ns(q->I.model.nsite, q->I.gs_up, q->I.gs_dn));
+        q->coef = Lease<double>(c->pool, (size_t)q->res[w].nstep);
+        CK(cudaMemcpyAsync(q->coef.p, q->res[w].coeff.data(), sizeof(double) * q->res[w].nstep,
+                           cudaMemcpyHostToDevice, c->stream));
+        q->phase = 2;
+    }
+    for (ServReq* q : eig) {                                  // normalise (lanczos_solver.f90:291), plan the runs
+        BatchInst& I = q->I;
+        const long long n = sector_dim_ns(I.model.nsite, I.gs_up, I.gs_dn);
+        launch_dot(I.gsvec.p, I.gsvec.p, n, c->dot_part->as<double>(), c->scal->as<double>(), c->stream);
+        launch_scale_inv_sqrt(I.gsvec.p, n, c->scal->as<double>(), c->stream);
+        g_launches += 3;
+        const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
+        q->runs = cluster_runs(I.model.norb, even, I.gs_up, I.gs_dn);
+        for (GreenRun& g : q->runs) {
+            g.mt = I.mt.get();
+            g.gs = I.gsvec.p;
+            g.gs_up = I.gs_up; g.gs_dn = I.gs_dn;
+            g.e0 = I.e0;
+        }
+        q->gab = Lease<double>(c->pool, std::max<size_t>(q->runs.size(), 1) * 2 * maxnstep);
+        CK(cudaMemsetAsync(q->gab.p, 0, sizeof(double) * std::max<size_t>(q->runs.size(), 1) * 2 * maxnstep,
+                           c->stream));
+        q->phase = 3;
+    }
+    CKLAUNCH();
+    if (!green.empty()) {                                     // continued fractions of all finishing requests
+        std::vector<CFJob> cj;
+        std::vector<std::pair<ServReq*, int>> cjr;
+        size_t ng = 0;
+        for (ServReq* q : green) ng += q->runs.size();
+        Lease<double> g(c->pool, std::max<size_t>(ng, 1) * 2 * nw);
+        CK(cudaMemsetAsync(g.p, 0, sizeof(double) * std::max<size_t>(ng, 1) * 2 * nw, c->stream));
+        size_t gi = 0;
+        for (ServReq* q : green)
+            for (size_t r = 0; r < q->runs.size(); r++, gi++) {
+                GreenRun& gr = q->runs[r];
+                if (gr.nstep < 0) {
+                    const JobSpec& j = specs[-1 - gr.nstep];
+                    gr.nstep = j.nstep;
+                    gr.norm0 = j.norm0;
+                }
+                if (gr.nstep < 1) continue;
+                CFJob J;
+                J.a = gr.a; J.b = gr.b;
+                J.b1 = gr.norm0;
+                J.levels = (gr.nstep == 1 && maxnstep >= 2) ? 2 : gr.nstep;
+                J.zr_shift = (gr.pm == 1) ? gr.e0 : -gr.e0;
+                J.sign = (gr.pm == 1) ? -1.0 : 1.0;
+                J.g = g.p + gi * 2 * nw;
+                cj.push_back(J);
+            }
+        if (!cj.empty()) {
+            Lease<CFJob> dj(c->pool, cj.size());
+            CK(cudaMemcpyAsync(dj.p, cj.data(), sizeof(CFJob) * cj.size(), cudaMemcpyHostToDevice, c->stream));
+            launch_cf(dj.p, (int)cj.size(), sv->omega->as<double>(), nw, c->stream);
+            g_launches += 1;
+            CKLAUNCH();
+        }
+        std::vector<double> hg(std::max<size_t>(ng, 1) * 2 * nw);
+        CK(cudaMemcpyAsync(hg.data(), g.p, sizeof(double) * hg.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        gi = 0;
+        for (ServReq* q : green) {
+            BatchInst& I = q->I;
+            std::vector<std::vector<double>> gs(q->runs.size()), abs_(q->runs.size());
+            for (size_t r = 0; r < q->runs.size(); r++, gi++)
+                gs[r].assign(hg.begin() + gi * 2 * nw, hg.begin() + (gi + 1) * 2 * nw);
+            const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
+            q->G.assign((size_t)2 * nw * I.model.norb * I.nspin, 0.0);
+            assemble_cluster(I.model.norb, I.nspin, even, maxnstep, nw, gs, abs_, 0, q->G.data(), nullptr);
+            q->phase = 4;
+        }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    int nfin = 0;                                             // retire finished requests, free their memory
+    for (auto it = sv->active.begin(); it != sv->active.end();) {
+        if ((*it)->phase == 4) {
+            ServReq& q = **it;
+            q.I.gsvec.reset(); q.I.mt.reset(); q.ab.reset(); q.coef.reset(); q.gab.reset();
+            sv->reserved -= q.I.footprint;
+            sv->finished[q.id] = std::move(*it);
+            it = sv->active.erase(it);
+            nfin++;
+        } else {
+            ++it;
+        }
+    }
+    return nfin;
 }
 
 template <class F>
@@ -1592,6 +1850,84 @@ int edzt_cluster_green_ftn(edzt_ctx* c, int nspin, int maxnstep, int nw, const d
         arg_check(G_cl != nullptr && (omega || nw == 0), "bad arguments");
         cluster_green_impl(c, nspin, maxnstep, nw, omega, G_cl, coeffs);
     });
+}
+
+int edzt_server_create(edzt_ctx* c, int maxnstep, int nw, const double* omega, size_t hbm_budget,
+                       edzt_server** out)
+{
+    if (!out) return EDZT_ERR_ARG;
+    *out = nullptr;
+    return guarded(c, [&] {
+        arg_check(maxnstep >= 1 && nw >= 0 && (nw == 0 || omega != nullptr), "maxnstep >= 1, nw >= 0, omega");
+        auto sv = std::make_unique<edzt_server>();
+        sv->c = c;
+        sv->maxnstep = maxnstep;
+        sv->nw = nw;
+        sv->omega = std::make_unique<DevBuf>(sizeof(double) * std::max(nw, 1));
+        if (nw > 0) CK(cudaMemcpy(sv->omega->p, omega, sizeof(double) * nw, cudaMemcpyDefault));
+        if (hbm_budget == 0) {
+            size_t fr = 0, tot = 0;
+            CK(cudaMemGetInfo(&fr, &tot));
+            hbm_budget = fr / 10 * 8;
+        }
+        sv->budget = (long long)hbm_budget;
+        *out = sv.release();
+    });
+}
+
+int edzt_server_submit(edzt_server* sv, const edzt_instance* inst, long long* id)
+{
+    if (!sv) return EDZT_ERR_ARG;
+    return guarded(sv->c, [&] {
+        arg_check(inst != nullptr && id != nullptr, "inst and id required");
+        auto q = std::make_unique<ServReq>();
+        init_inst(*inst, q->I);
+        q->id = sv->next_id++;
+        *id = q->id;
+        sv->queue.push_back(std::move(q));
+    });
+}
+
+int edzt_server_step(edzt_server* sv, int* nactive, int* nqueued, int* nfinished)
+{
+    if (!sv) return EDZT_ERR_ARG;
+    return guarded(sv->c, [&] {
+        const int nf = server_step(sv);
+        if (nfinished) *nfinished = nf;
+        if (nactive) *nactive = (int)sv->active.size();
+        if (nqueued) *nqueued = (int)sv->queue.size();
+    });
+}
+
+int edzt_server_result(edzt_server* sv, long long id, int* done, int* isector, double* e0, double* G_cl)
+{
+    if (!sv) return EDZT_ERR_ARG;
+    return guarded(sv->c, [&] {
+        arg_check(done != nullptr, "done required");
+        auto it = sv->finished.find(id);
+        *done = 0;
+        if (it == sv->finished.end()) return;
+        ServReq& q = *it->second;
+        if (!q.error.empty()) {
+            const std::string msg = "request " + std::to_string(id) + ": " + q.error;
+            sv->finished.erase(it);
+            throw EdztError{EDZT_ERR_NUMERIC, msg};
+        }
+        *done = 1;
+        if (isector) *isector = q.I.best;
+        if (e0) *e0 = q.I.e0;
+        if (G_cl && !q.G.empty()) copy_out(sv->c, G_cl, q.G.data(), sizeof(double) * q.G.size());
+        CK(cudaStreamSynchronize(sv->c->stream));
+        sv->finished.erase(it);
+    });
+}
+
+void edzt_server_destroy(edzt_server* sv)
+{
+    if (!sv) return;
+    cudaSetDevice(sv->c->device);
+    cudaStreamSynchronize(sv->c->stream);
+    delete sv;
 }
 
 int edzt_solve_batch(edzt_ctx* c, int ninst, const edzt_instance* inst, int maxnstep, int nw, const double* omega,

@@ -185,6 +185,31 @@ typedef struct edzt_instance {
 int edzt_solve_batch(edzt_ctx *ctx, int ninst, const edzt_instance *inst, int maxnstep, int nw,
                      const double *omega, int *isector, double *e0, double *G_cl, size_t hbm_budget);
 
+/* Served form: continuous batching of impurity solves on one context.
+ * Requests (edzt_instance, copied at submit) wait in a queue and are
+ * admitted by their device-memory footprint (the sector scan's 32 B per
+ * state, or the Green's runs') while the admitted ones fit hbm_budget (0: 80%
+ * of the free memory; a request is always admitted when nothing else runs).
+ * Every edzt_server_step runs one persistent launch carrying the current
+ * phase of every admitted request -- sector scan, eigenvector pass, or c / c^+
+ * runs plus continued fractions -- so each request finishes in three steps
+ * and requests submitted meanwhile join at the next step.  A request's result
+ * is the same as edzt_solve's on it alone, to rounding.  maxnstep, nw, omega
+ * are fixed per server; destroy the server before its context. */
+typedef struct edzt_server edzt_server;
+int edzt_server_create(edzt_ctx *ctx, int maxnstep, int nw, const double *omega, size_t hbm_budget,
+                       edzt_server **out);
+/* Queues one request; *id identifies it. */
+int edzt_server_submit(edzt_server *srv, const edzt_instance *inst, long long *id);
+/* Admits what fits and advances every admitted request by one phase (blocks
+ * until the step's GPU work is done).  nactive, nqueued, nfinished nullable. */
+int edzt_server_step(edzt_server *srv, int *nactive, int *nqueued, int *nfinished);
+/* *done = 1 and the results (isector, e0, G_cl(nw, norb, nspin) complex; all
+ * nullable) once request id has finished, which also releases it; *done = 0
+ * while it runs. */
+int edzt_server_result(edzt_server *srv, long long id, int *done, int *isector, double *e0, double *G_cl);
+void edzt_server_destroy(edzt_server *srv);
+
 /* Kernel launches issued by this context since creation (instrumentation). */
 long long edzt_launch_count(const edzt_ctx *ctx);
 
