@@ -20,6 +20,14 @@ and seeded: the reference quotes no data set.
              this host's cores, on a bounded sample of the workload
   plain_gpu  the reference's Lanczos structure run kernel by kernel on the
              same GPU (the one-solve-at-a-time drop-in comparator)
+  batched    the batched form (one GPU): the first --batched instances of the
+             seeded 256-instance draw (nsite ~ U{8..14}) in one
+             edzt_solve_batch call, solves/s, with the plain engine's solves/s
+             on the same instances (one per nsite timed, weighted by counts)
+  served     the served form (one GPU): --served requests, Poisson arrivals at
+             200/s, nsite 8..12, through edzt_server's request loop: solves/s
+             and p50/p99 latency from arrival to result, with the plain
+             engine's solves/s on the same requests
 
 --impl reference times the CPU oracle on all host threads (the reference
 itself is Fortran + MPI + MKL and cannot be built here).
@@ -138,6 +146,93 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU legs (the oracle: test infrastructure, used here only as the baseline)
 # ---------------------------------------------------------------------------
+def plain_estimate(pkg, s, items, omega, maxnstep):
+    """Plain one-solve-at-a-time GPU engine time per solve, measured on one
+    item per nsite and weighted by the items' nsite counts."""
+    import numpy as np
+    import torch
+    by_ns = {}
+    for it in items:
+        by_ns.setdefault(it["model"].nsite, []).append(it)
+    s.set_engine(pkg.ENGINE_PLAIN)
+    total = 0.0
+    per_ns = {}
+    try:
+        for ns, group in sorted(by_ns.items()):
+            it = group[0]
+            s.set_model(it["model"])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.solve(it["sectors"], maxnstep, omega, nspin=it.get("nspin", 1), seed=it.get("seed", 0))
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            per_ns[int(ns)] = round(1000 * dt, 2)
+            total += dt * len(group)
+    finally:
+        s.set_engine(pkg.ENGINE_FUSED)
+    return len(items) / total, per_ns
+
+
+def batched_leg(pkg, s, cfgs, n):
+    """The batched form: the first n instances of the seeded 256-instance draw
+    (nsite ~ U{8..14}, 9 or 4 sectors within one electron of half filling,
+    nspin 2: 4 c/c^+ runs each), one edzt_solve_batch call."""
+    import numpy as np
+    import torch
+    insts = cfgs.batch(256)[:n]
+    omega = pkg.matsubara(2048, 100.0)
+    s.solve_batch(insts[:2], 300, omega)                     # warm-up (tables, pool)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.solve_batch(insts, 300, omega)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    plain, per_ns = plain_estimate(pkg, s, insts, omega, 300)
+    hist = np.bincount([i["model"].nsite for i in insts], minlength=15)[8:15].tolist()
+    return {"value": n / dt, "unit": "solves/s", "instances": n, "seconds": dt,
+            "nsite_counts_8_to_14": hist, "plain_gpu": {"value": plain, "unit": "solves/s",
+                                                        "ms_per_solve_by_nsite": per_ns,
+                                                        "how": "one instance per nsite timed, weighted by counts"},
+            "sample": f"first {n} of the 256 seeded instances (seed 4), wall clock of one call, synchronised"}
+
+
+def served_leg(pkg, s, cfgs, n, seed=5):
+    """The served form: n requests with Poisson arrivals (mean 200 req/s),
+    nsite ~ U{8..12}, random U, J = 0, bath as the batched form, nspin 2,
+    through edzt_server's request loop."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    omega = pkg.matsubara(2048, 100.0)
+    reqs = []
+    for _ in range(n):
+        ns = int(rng.integers(8, 13))
+        nb = ns - 1
+        U = float(rng.uniform(1.0, 4.0))
+        ek = rng.uniform(-2.0, 2.0, nb)
+        V = rng.uniform(0.1, 1.0, nb)
+        m = pkg.Model(1, nb, np.zeros((1, 2)), np.stack([ek, ek], 1), np.stack([V, V], 1).reshape(1, nb, 2),
+                      U=U, mu=U / 2)
+        reqs.append(dict(model=m, sectors=cfgs.near_half_sectors(ns), nspin=2, seed=int(rng.integers(1 << 40))))
+    arrivals = np.cumsum(rng.exponential(1.0 / 200.0, n))
+    arrivals -= arrivals[0]
+    sv = pkg.Server(s, 300, omega)
+    try:
+        sv.submit(reqs[0])
+        for _ in range(4):                                   # warm-up
+            sv.step()
+        _, lat, total = pkg.serve(sv, reqs, arrivals)
+    finally:
+        sv.close()
+    plain, per_ns = plain_estimate(pkg, s, reqs, omega, 300)
+    return {"value": n / total, "unit": "solves/s", "requests": n, "seconds": total,
+            "latency_ms": {"p50": float(np.percentile(lat, 50) * 1000), "p99": float(np.percentile(lat, 99) * 1000)},
+            "offered_rate_per_s": 200.0,
+            "plain_gpu": {"value": plain, "unit": "solves/s", "ms_per_solve_by_nsite": per_ns,
+                          "how": "one request per nsite timed, weighted by counts"},
+            "sample": f"{n} requests, nsite 8..12 of the 8..16 distribution (nsite 13..16 solves take seconds "
+                      "each and do not fit the bench's time bound), Poisson 200/s (seed 5)"}
+
+
 def read_traffic(path):
     """DRAM bytes per k_lanczos launch (dram__bytes_read.sum + dram__bytes_write.sum
     from one ncu capture of this workload), from the `bytes_per_launch:` line of
@@ -345,6 +440,14 @@ def run_gpu(args):
                         "and Green's-function launches (<= 27 MB) are L2-resident"}
     roofline["traffic"] = read_traffic(args.traffic_file)
 
+    batched = served = None
+    if world == 1 and args.batched > 0:
+        cfgs = importlib.import_module("dmft_ed_zt_b200.configs")
+        batched = batched_leg(pkg, s, cfgs, args.batched)
+    if world == 1 and args.served > 0:
+        cfgs = importlib.import_module("dmft_ed_zt_b200.configs")
+        served = served_leg(pkg, s, cfgs, args.served)
+
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         v, cores, sample, _ = cpu_solve_sample(cfg)
@@ -359,7 +462,7 @@ def run_gpu(args):
                 "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)),
                                "p99": float(np.percentile(lat_sorted, 99))},
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
-                "plain_gpu": plain, "clocks": clk, "e0": e0.value}
+                "plain_gpu": plain, "batched": batched, "served": served, "clocks": clk, "e0": e0.value}
         print(json.dumps(line))
     s.close()
     if dist is not None:
@@ -376,6 +479,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--batched", type=int, default=64, help="instances of the batched leg (0: skip)")
+    ap.add_argument("--served", type=int, default=32, help="requests of the served leg (0: skip)")
     ap.add_argument("--traffic-file", default=os.path.join(ROOT, "profiles", "k_lanczos_aim_n12_dram.txt"))
     args = ap.parse_args()
     if args.impl == "reference":

@@ -515,10 +515,18 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     int block = 256;
     const int G = persistent_grid(c, smem, &block);
     if (G <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
-    for (int j = 0; j < nj; j++) {   // fewer rows per tile where that evens a job out over the grid
-        LzJob& J = jobs[j];
-        J.rows = lz_rows_balanced(J.S.dn.count, J.rows, G);
-        J.ntiles = (J.S.dn.count + J.rows - 1) / J.rows;
+    // A launch with few tiles (one or a few sectors) spreads each job evenly
+    // over the grid with smaller tiles; a launch with many (a batch) keeps
+    // the largest tiles, since every tile costs a staging round and two CTA
+    // barriers whatever its size.
+    long long tiles_max = 0;
+    for (int j = 0; j < nj; j++) tiles_max += jobs[j].ntiles;
+    if (tiles_max < 4LL * G) {
+        for (int j = 0; j < nj; j++) {
+            LzJob& J = jobs[j];
+            J.rows = lz_rows_balanced(J.S.dn.count, J.rows, G);
+            J.ntiles = (J.S.dn.count + J.rows - 1) / J.rows;
+        }
     }
     // tiles of all jobs in one list; CTA b takes tiles b, b+G, ...; the
     // participants of job j are CTAs (tile0 + q) mod G, q < min(G, ntiles)
