@@ -295,6 +295,7 @@ DevSector make_sector_mt(edzt_ctx* c, ModelTables& mt, int nu, int nd)
     fill(S.up, su, ou);
     fill(S.dn, sd, od);
     S.dim = (long long)su.count * sd.count;
+    arg_check(S.dim < (1LL << 32), "sector dimension must stay below 2^32 states");
     S.P = mt.P;
     S.has_j = mt.has_j ? 1 : 0;
     S.wint = mt.wint->as<double>();

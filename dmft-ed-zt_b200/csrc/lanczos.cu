@@ -360,27 +360,83 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
         }
         stage_rows(sJ.S.dn, C, r0, rows);
         __syncthreads();
-        const SrcPairs src{YWp, am};
-        int r = threadIdx.x / nup, iu = threadIdx.x - r * nup;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            const double xe = C.xs[e];
-            const double wprev = FIRST ? 0.0 : __ldcg(reinterpret_cast<const double*>(Yt + e) + 1);
-            double du, dv;
-            hv_elem(sJ.S, C, wint, amp, src, r, iu, xe, du, dv);
-            double hv = du + (FIRST ? dv / b_cur : dv * rb);     // sum c * w_k(id', iu)
-            if (sJ.S.has_j) hv = hv_exchange(sJ.S, C, r, iu, hv, fetch);
-            const double y = FIRST ? hv : fma(mb, wprev, hv);
-            __stcg(Ot + e, make_double2(y, xe));
-            if (coeff) {
-                const double t = fma(am, xe, y);         // y - a_{k-1} w (a_0 = 0)
-                acc[0] = fma(xe, t, acc[0]);
-                acc[1] = fma(t, t, acc[1]);
-                acc[2] = fma(xe, xe, acc[2]);
-            } else {
-                __stcg(Et + e, FIRST ? ck * xe : fma(ck, xe, __ldcg(Et + e)));
+        // Warps take (row, column segment) items; a row's down hops, energy and
+        // impurity bits are loaded once per item into registers, and the warp
+        // walks its segment 32 columns at a time.
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+        const int W = max(32, ((nup + nwarps - 1) / nwarps + 31) & ~31);
+        const int nseg = (nup + W - 1) / W;
+        const uint4* __restrict__ hpk = sJ.S.up.hpk;
+        const bool two = sJ.S.up.hw > 4;
+        for (int item = warp; item < rows * nseg; item += nwarps) {
+            const int r = item / nseg, c0 = (item - r * nseg) * W, c1 = min(nup, c0 + W);
+            const int hd = C.dcnt[r];
+            EDZT_OK_OR(hd >= 0 && hd <= C.hw, 13, r, hd, C.hw, continue)
+            const DHop* __restrict__ rec = C.dh + r * C.hw;
+            unsigned off[8];                                         // amplitudes stay in shared memory
+#pragma unroll
+            for (int q = 0; q < 8; q++) off[q] = (q < hd) ? (unsigned)rec[q].off : 0u;
+            const double rowe = C.de1[r];
+            const double* __restrict__ wrow = wint + C.dimp[r];
+            const double* __restrict__ xrow = C.xs + r * nup;
+            for (int iu = c0 + lane; iu < c1; iu += 32) {
+                const int e = r * nup + iu;
+                const double2* __restrict__ col = YWp + iu;
+                // every load of the element first
+                const uint4 q0 = __ldg(hpk + iu);
+                const uint4 q1 = two ? __ldg(hpk + nup + iu) : make_uint4(0u, 0u, 0u, 0u);
+                const int hu = __ldg(sJ.S.up.hcnt + iu);
+                const int pu = __ldg(sJ.S.up.imp + iu);
+                const double e1u = __ldg(sJ.S.up.e1 + iu);
+                const double wprev = FIRST ? 0.0 : __ldcg(reinterpret_cast<const double*>(Yt + e) + 1);
+                const double eprev = (coeff || FIRST) ? 0.0 : __ldcg(Et + e);
+                double2 g[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    EDZT_OK_OR(q >= hd || (long long)off[q] + iu < sJ.S.dim, 21, off[q], iu, sJ.S.dim, g[q] = make_double2(0.0, 0.0); continue)
+                    g[q] = (q < hd) ? __ldcg(col + off[q]) : make_double2(0.0, 0.0);
+                }
+                // diagonal and up hops from the staged row
+                const double xe = xrow[iu];
+                double hv = (e1u + rowe + wrow[pu * sJ.S.P]) * xe;
+                const uint32_t eu[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    if (c < hu) {
+                        EDZT_OK_OR(edzt_hop_rank(eu[c]) < nup && edzt_hop_slot(eu[c]) < sJ.S.up.namp, 11, iu, c,
+                                   (long long)eu[c], continue)
+                        hv = fma(amp[edzt_hop_slot(eu[c])], xrow[edzt_hop_rank(eu[c])], hv);
+                    }
+                }
+                for (int h0 = 8; h0 < hu; h0 += 4) {                 // hop lists longer than 8
+                    const uint4 q = __ldg(hpk + (size_t)(h0 >> 2) * nup + iu);
+                    const uint32_t f[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        if (h0 + c < hu) hv = fma(amp[edzt_hop_slot(f[c])], xrow[edzt_hop_rank(f[c])], hv);
+                }
+                // down hops: v = y - a w at each neighbour, as its owner forms it
+                double dv = 0.0;
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    if (q < hd) dv = fma(rec[q].val, fma(am, g[q].y, g[q].x), dv);
+                for (int h = 8; h < hd; h++) {
+                    const double2 gg = __ldcg(col + rec[h].off);
+                    dv = fma(rec[h].val, fma(am, gg.y, gg.x), dv);
+                }
+                hv += FIRST ? dv / b_cur : dv * rb;                   // sum c * w_k(id', iu)
+                if (sJ.S.has_j) hv = hv_exchange(sJ.S, C, r, iu, hv, fetch);
+                const double y = FIRST ? hv : fma(mb, wprev, hv);
+                __stcg(Ot + e, make_double2(y, xe));
+                if (coeff) {
+                    const double t = fma(am, xe, y);         // y - a_{k-1} w (a_0 = 0)
+                    acc[0] = fma(xe, t, acc[0]);
+                    acc[1] = fma(t, t, acc[1]);
+                    acc[2] = fma(xe, xe, acc[2]);
+                } else {
+                    __stcg(Et + e, FIRST ? ck * xe : fma(ck, xe, eprev));
+                }
             }
-            iu += blockDim.x;
-            while (iu >= nup) { iu -= nup; ++r; }
         }
         __syncthreads();
     };
