@@ -49,7 +49,7 @@ EXPORTS = (
     "edzt_lanczos_iteration", "edzt_diag_lanczos", "edzt_ground_state", "edzt_gs_dim",
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
     "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
-    "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
+    "edzt_cluster_green_matrix", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
 )
 # Limits of edzt_lanczos_iteration_noalloc (its static scratch array).
 NOALLOC_MAX_DIM = 262144
@@ -119,6 +119,7 @@ def load_library(path: str = LIB_PATH):
     L.edzt_apply_c.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_int, _vp]
     L.edzt_lanczos_iteration.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
     L.edzt_lanczos_iteration_noalloc.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
+    L.edzt_cluster_green_matrix.argtypes = [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp]
     L.edzt_solve_batch.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_size_t]
     L.edzt_server_create.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_size_t, C.POINTER(C.c_void_p)]
     L.edzt_server_submit.argtypes = [_vp, _vp, C.POINTER(C.c_longlong)]
@@ -347,6 +348,17 @@ class Solver:
                                                    _ptr(coeffs)))
         Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, norb, nw)
         return dict(G_cl=Gc, coeffs=coeffs.reshape(norb, 2, 4, maxnstep))
+
+    def cluster_green_matrix(self, nspin, maxnstep, omega):
+        """Full G_ab on the resident ground state (edzt_cluster_green_matrix),
+        returned as G[ispin, a, b, iw]."""
+        omega = _f64(omega)
+        nw = omega.size
+        norb = self.model.norb
+        G = np.zeros(2 * nw * norb * norb * nspin)
+        self._check(self._L.edzt_cluster_green_matrix(self._h, nspin, maxnstep, nw, _ptr(omega), _ptr(G)))
+        Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, norb, norb, nw)   # [s, b, a, iw]
+        return Gc.transpose(0, 2, 1, 3)
 
     def solve_batch(self, instances, maxnstep, omega, hbm_budget=0):
         """Many independent solves in batched persistent launches

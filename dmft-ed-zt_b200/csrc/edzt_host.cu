@@ -832,6 +832,7 @@ struct GreenRun {
     const double* gs = nullptr;    // ground state of the run's model (device), sector (gs_up, gs_dn)
     int gs_up = 0, gs_dn = 0;
     double e0 = 0.0;
+    const double* start = nullptr; // explicit start vector (device) instead of c^(+)|gs>, e.g. (c_a + c_b)^(+)|gs>
     int iorb, ispin, pm;
     int nu, nd;            // excitation sector
     int nstep = 0;
@@ -896,9 +897,14 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
             s.mt = g.mt;
             s.nu = g.nu; s.nd = g.nd;
             s.mode = LZ_COEFF;
-            s.init = LZ_INIT_APPLYC;
-            s.ac = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
-            s.ac_src = g.gs;
+            if (g.start) {
+                s.init = LZ_INIT_COPY;
+                s.ac_src = g.start;
+            } else {
+                s.init = LZ_INIT_APPLYC;
+                s.ac = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
+                s.ac_src = g.gs;
+            }
             s.maxnstep = maxnstep;
             s.a = g.a; s.b = g.b;
             specs.push_back(s);
@@ -916,8 +922,12 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
             if (sector_dim_ns(ns, g.nu, g.nd) <= 0) continue;
             DevSector S = make_sector_mt(c, *g.mt, g.nu, g.nd);
             Lease<double> vin(c->pool, (size_t)S.dim);
-            ApplyCArgs A = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
-            launch_apply_c(A, g.gs, vin.p, c->stream);
+            if (g.start) {
+                launch_copy(vin.p, g.start, S.dim, c->stream);
+            } else {
+                ApplyCArgs A = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
+                launch_apply_c(A, g.gs, vin.p, c->stream);
+            }
             g_launches += 1;
             std::vector<double> ha(maxnstep), hb(maxnstep);
             g.nstep = plain_lanczos(c, S, vin.p, maxnstep, ha.data(), hb.data(), &g.norm0, nullptr, nullptr);
@@ -1075,6 +1085,94 @@ void green_diag_impl(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, con
     copy_out(c, am, abs_[1].data(), sizeof(double) * maxnstep);
     copy_out(c, bm, abs_[1].data() + maxnstep, sizeof(double) * maxnstep);
     copy_out(c, g, gsum.data(), sizeof(double) * 2 * nw);
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+// The full cluster Green's function matrix G_ab(nw, norb, norb, nspin) on the
+// resident ground state.  Beyond the reference, which computes the diagonal
+// only (dmft_green.f90:71-121): G_ab = (G_(a+b) - G_aa - G_bb) / 2, where
+// G_(a+b) is green_diag's construction for the operator c_a + c_b, i.e. its
+// c^+ and c runs start from (c_a^+ + c_b^+)|gs> and (c_a + c_b)|gs>.  The
+// diagonal and spin rules are cluster_green_ftn's (:76-80, :111-118).
+void cluster_green_matrix_impl(edzt_ctx* c, int nspin, int maxnstep, int nw, const double* omega, double* G)
+{
+    require_model(c);
+    require_gs(c);
+    arg_check(nspin == 1 || nspin == 2, "nspin must be 1 or 2");
+    arg_check(maxnstep >= 1 && nw >= 0, "maxnstep >= 1, nw >= 0");
+    const int norb = c->mt.model.norb, ns = nsite_of(c);
+    const bool even = !(nspin == 2 || c->gs_up != c->gs_dn);
+    const int nsp = even ? 1 : 2;
+    std::vector<GreenRun> runs = cluster_runs(norb, even, c->gs_up, c->gs_dn);   // the diagonal, order (a, spin, pm)
+    const size_t ndiag = runs.size();
+    std::vector<Lease<double>> starts;
+    struct Pair { int a, b, ispin; size_t r; };
+    std::vector<Pair> pairs;
+    for (int ispin = 1; ispin <= nsp; ispin++)
+        for (int a = 1; a <= norb; a++)
+            for (int b = a + 1; b <= norb; b++) {
+                pairs.push_back({a, b, ispin, runs.size()});
+                for (int pm = 1; pm <= 2; pm++) {
+                    GreenRun g;
+                    g.iorb = a; g.ispin = ispin; g.pm = pm;
+                    excitation(c->gs_up, c->gs_dn, pm, ispin, &g.nu, &g.nd);
+                    const long long n = sector_dim_ns(ns, g.nu, g.nd);
+                    if (n > 0) {     // (c_a + c_b)^(+)|gs> = c_a^(+)|gs> + c_b^(+)|gs>
+                        starts.emplace_back(c->pool, (size_t)n);
+                        Lease<double> tmp(c->pool, (size_t)n);
+                        launch_apply_c(applyc_args(c, c->gs_up, c->gs_dn, pm, a, ispin, g.nu, g.nd), c->gs_vec.p,
+                                       starts.back().p, c->stream);
+                        launch_apply_c(applyc_args(c, c->gs_up, c->gs_dn, pm, b, ispin, g.nu, g.nd), c->gs_vec.p,
+                                       tmp.p, c->stream);
+                        launch_axpy(starts.back().p, tmp.p, n, nullptr, 1.0, 1.0, c->stream);
+                        g_launches += 3;
+                        CK(cudaStreamSynchronize(c->stream));   // tmp goes back to the pool
+                        g.start = starts.back().p;
+                    }
+                    runs.push_back(g);
+                }
+            }
+    CKLAUNCH();
+    InVec om(c, omega, nw);
+    std::vector<std::vector<double>> gs, abs_;
+    green_runs(c, runs, maxnstep, nw, om.d, gs, abs_);
+    // g[spin][a][b] per frequency: the diagonal from the single runs, the rest from the pairs
+    std::vector<double> gm((size_t)nsp * norb * norb * 2 * nw, 0.0);
+    auto at = [&](int sp, int a, int b) { return gm.data() + (((size_t)sp * norb + a) * norb + b) * 2 * nw; };
+    size_t r = 0;
+    for (int a = 0; a < norb; a++)
+        for (int sp = 0; sp < nsp; sp++)
+            for (int pm = 1; pm <= 2; pm++, r++)
+                for (int q = 0; q < 2 * nw; q++) at(sp, a, a)[q] += gs[r][q];
+    (void)ndiag;
+    for (const Pair& P : pairs) {
+        const int sp = P.ispin - 1, a = P.a - 1, b = P.b - 1;
+        for (int q = 0; q < 2 * nw; q++) {
+            const double gab = gs[P.r][q] + gs[P.r + 1][q];
+            const double v = 0.5 * (gab - at(sp, a, a)[q] - at(sp, b, b)[q]);
+            at(sp, a, b)[q] = v;
+            at(sp, b, a)[q] = v;
+        }
+    }
+    // G(nw, norb, norb, nspin), column-major, complex interleaved (the spin rule of :111-118)
+    std::vector<double> Gh((size_t)2 * nw * norb * norb * nspin, 0.0);
+    for (int s = 0; s < nspin; s++)
+        for (int b = 0; b < norb; b++)
+            for (int a = 0; a < norb; a++)
+                for (int iw = 0; iw < nw; iw++) {
+                    const size_t o = 2 * ((size_t)iw + (size_t)nw * (a + (size_t)norb * (b + (size_t)norb * s)));
+                    double re, im;
+                    if (even) {
+                        re = at(0, a, b)[2 * iw]; im = at(0, a, b)[2 * iw + 1];
+                    } else if (nspin == 1) {
+                        re = 0.5 * (at(0, a, b)[2 * iw] + at(1, a, b)[2 * iw]);
+                        im = 0.5 * (at(0, a, b)[2 * iw + 1] + at(1, a, b)[2 * iw + 1]);
+                    } else {
+                        re = at(s, a, b)[2 * iw]; im = at(s, a, b)[2 * iw + 1];
+                    }
+                    Gh[o] = re; Gh[o + 1] = im;
+                }
+    copy_out(c, G, Gh.data(), sizeof(double) * Gh.size());
     CK(cudaStreamSynchronize(c->stream));
 }
 
@@ -1849,6 +1947,14 @@ int edzt_green_diag(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, cons
     return guarded(c, [&] {
         arg_check(ap && bp && am && bm && g && (omega || nw == 0), "bad arguments");
         green_diag_impl(c, iorb, ispin, maxnstep, nw, omega, ap, bp, am, bm, g);
+    });
+}
+
+int edzt_cluster_green_matrix(edzt_ctx* c, int nspin, int maxnstep, int nw, const double* omega, double* G)
+{
+    return guarded(c, [&] {
+        arg_check(G != nullptr && (omega || nw == 0), "bad arguments");
+        cluster_green_matrix_impl(c, nspin, maxnstep, nw, omega, G);
     });
 }
 

@@ -155,6 +155,15 @@ int edzt_green_diag(edzt_ctx *ctx, int iorb, int ispin, int maxnstep, int nw, co
 int edzt_cluster_green_ftn(edzt_ctx *ctx, int nspin, int maxnstep, int nw, const double *omega,
                            double *G_cl, double *coeffs);
 
+/* Full cluster Green's function matrix on the resident ground state:
+ * G(nw, norb, norb, nspin) complex (column-major, interleaved).  No
+ * counterpart in the reference, which computes the diagonal only
+ * (src/dmft_green.f90:71-121): G_ab = (G_(a+b) - G_aa - G_bb) / 2 with
+ * G_(a+b) green_diag's construction for c_a + c_b (c^+ and c runs from
+ * (c_a^+ + c_b^+)|gs> and (c_a + c_b)|gs>), diagonal and spin rules as
+ * edzt_cluster_green_ftn. */
+int edzt_cluster_green_matrix(edzt_ctx *ctx, int nspin, int maxnstep, int nw, const double *omega, double *G);
+
 /* One impurity solve: edzt_ground_state followed by edzt_cluster_green_ftn
  * (the calls at src/dmft.f90:76-78).  G_cl and coeffs nullable. */
 int edzt_solve(edzt_ctx *ctx, int nsector, const int *sectors, int maxnstep, uint64_t seed, int nspin,

@@ -267,6 +267,66 @@ class Oracle:
         Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, self.norb, nw)   # (ispin, iorb, iw)
         return dict(G_cl=Gc, coeffs=coeffs.reshape(self.norb, 2, 4, maxnstep))
 
+    def green_run(self, v_init, nu, nd, pm, e0, maxnstep, omega):
+        """One c^+ (pm=1) or c (pm=2) run of green_diag (dmft_green.f90:204-257)
+        from an explicit start vector in sector (nu, nd): Lanczos, b(1) =
+        |v_init|, continued fraction on E0 + i w (c^+) or -E0 + i w (c)."""
+        n, a, b = self.lanczos_iteration(nu, nd, v_init, maxnstep)
+        g = np.zeros(len(omega), dtype=complex)
+        if n < 1:
+            return g
+        b = b.copy()
+        b[0] = np.sqrt(dot(v_init, v_init))
+        nl = 2 if (n == 1 and maxnstep >= 2) else n
+        for i, w in enumerate(omega):
+            if pm == 1:
+                g[i] = continued_fraction(complex(e0, w), nl, a, b, -1)
+            else:
+                g[i] = continued_fraction(complex(-e0, w), nl, a, b, +1)
+        return g
+
+    def cluster_green_matrix(self, nspin, ne_up, ne_dn, gsvec, e0, maxnstep, omega):
+        """The full G_ab(ispin, a, b, iw): the diagonal as cluster_green_ftn,
+        G_ab = (G_(a+b) - G_aa - G_bb) / 2 with G_(a+b) from runs on
+        (c_a + c_b)^(+)|gs> (an extension beyond the reference, which
+        computes the diagonal only, dmft_green.f90:71-121)."""
+        norb = self.norb
+        even = not (nspin == 2 or ne_up != ne_dn)
+        nsp = 1 if even else 2
+        gm = np.zeros((nsp, norb, norb, len(omega)), dtype=complex)
+
+        def exc(pm, ispin):
+            d = 1 if pm == 1 else -1
+            return ne_up + (d if ispin == 1 else 0), ne_dn + (d if ispin == 2 else 0)
+
+        def start(pm, orbs, ispin):
+            v = None
+            for a in orbs:
+                w = self.apply_c(ne_up, ne_dn, gsvec, pm, a, ispin)
+                v = w if v is None else v + w
+            return v
+
+        for sp in range(nsp):
+            for a in range(norb):
+                for pm in (1, 2):
+                    nu, nd = exc(pm, sp + 1)
+                    if self.dim(nu, nd) > 0:
+                        gm[sp, a, a] += self.green_run(start(pm, [a + 1], sp + 1), nu, nd, pm, e0, maxnstep, omega)
+            for a in range(norb):
+                for b in range(a + 1, norb):
+                    gab = np.zeros(len(omega), dtype=complex)
+                    for pm in (1, 2):
+                        nu, nd = exc(pm, sp + 1)
+                        if self.dim(nu, nd) > 0:
+                            gab += self.green_run(start(pm, [a + 1, b + 1], sp + 1), nu, nd, pm, e0, maxnstep,
+                                                  omega)
+                    gm[sp, a, b] = gm[sp, b, a] = 0.5 * (gab - gm[sp, a, a] - gm[sp, b, b])
+        if even:
+            return np.repeat(gm, nspin, axis=0)
+        if nspin == 1:
+            return 0.5 * (gm[0:1] + gm[1:2])
+        return gm
+
     def dense_h(self, ne_up, ne_dn) -> np.ndarray:
         """H assembled column by column from hx (the idea of debug.f90:13-57)."""
         n = self.dim(ne_up, ne_dn)

@@ -167,3 +167,44 @@ def test_solve_aim_n12(solver, configs, oracle_mod):
     r = solver.solve(cfg["sectors"], cfg["maxnstep"], omega, nspin=1, seed=0)
     assert r["isector"] == gs_ref["isector"] and _e_ok(r["e0"], gs_ref["e0"])
     assert np.abs(r["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
+
+
+@pytest.mark.parametrize("nspin", [1, 2])
+def test_cluster_green_matrix_kanamori(solver, configs, oracle_mod, nspin):
+    """Full G_ab of the two-orbital workload (200 steps) against the oracle's
+    restatement of the (c_a + c_b) construction; the diagonal equals
+    cluster_green_ftn's and the matrix is symmetric."""
+    cfg = configs.kanamori_n10()
+    o = oracle_for(oracle_mod, cfg["model"])
+    gs_ref = o.ground_state(cfg["sectors"], cfg["maxnstep"], seed=1)
+    omega = oracle_mod.matsubara(64, cfg["beta"])
+    nu, nd = gs_ref["sector"]
+    ref = o.cluster_green_matrix(nspin, nu, nd, gs_ref["vec"], gs_ref["e0"], cfg["maxnstep"], omega)
+    solver.set_model(cfg["model"])
+    solver.ground_state(cfg["sectors"], cfg["maxnstep"], seed=1)
+    G = solver.cluster_green_matrix(nspin, cfg["maxnstep"], omega)
+    assert G.shape == ref.shape == (nspin, 2, 2, 64)
+    assert np.abs(G - ref).max() <= G_TOL
+    assert np.abs(G - G.transpose(0, 2, 1, 3)).max() == 0.0
+    diag = solver.cluster_green_ftn(nspin, cfg["maxnstep"], omega)["G_cl"]     # (nspin, norb, nw)
+    for a in range(2):
+        assert np.abs(G[:, a, a] - diag[:, a]).max() <= G_TOL
+    # every bath site couples to one orbital here, so G_12 vanishes by symmetry
+    assert np.abs(G[:, 0, 1]).max() < 1e-9
+
+
+def test_cluster_green_matrix_coupled_orbitals(pkg, solver, oracle_mod):
+    """A two-orbital model whose bath sites hybridise with both orbitals:
+    G_12 is non-zero and matches the oracle."""
+    rng = np.random.default_rng(66)
+    m = random_model(pkg, rng, 2, 4, J=0.5, spin_dep=True)
+    sectors = [(u, 6 - u) for u in range(1, 6)]
+    o = oracle_for(oracle_mod, m)
+    gs_ref = o.ground_state(sectors, 150, seed=2)
+    omega = oracle_mod.matsubara(64, 20.0)
+    ref = o.cluster_green_matrix(2, *gs_ref["sector"], gs_ref["vec"], gs_ref["e0"], 150, omega)
+    solver.set_model(m)
+    solver.ground_state(sectors, 150, seed=2)
+    G = solver.cluster_green_matrix(2, 150, omega)
+    assert np.abs(G - ref).max() <= G_TOL
+    assert np.abs(G[:, 0, 1]).max() > 1e-3
