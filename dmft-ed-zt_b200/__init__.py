@@ -49,7 +49,7 @@ EXPORTS = (
     "edzt_lanczos_iteration", "edzt_diag_lanczos", "edzt_ground_state", "edzt_gs_dim",
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
     "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
-    "edzt_cluster_green_matrix", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
+    "edzt_cluster_green_matrix", "edzt_gs_occupancy", "edzt_green_real", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
 )
 # Limits of edzt_lanczos_iteration_noalloc (its static scratch array).
 NOALLOC_MAX_DIM = 262144
@@ -120,6 +120,8 @@ def load_library(path: str = LIB_PATH):
     L.edzt_lanczos_iteration.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
     L.edzt_lanczos_iteration_noalloc.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _ip, _vp, _vp]
     L.edzt_cluster_green_matrix.argtypes = [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp]
+    L.edzt_gs_occupancy.argtypes = [_vp, C.c_int, _vp, _vp]
+    L.edzt_green_real.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_double, _vp]
     L.edzt_solve_batch.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_size_t]
     L.edzt_server_create.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_size_t, C.POINTER(C.c_void_p)]
     L.edzt_server_submit.argtypes = [_vp, _vp, C.POINTER(C.c_longlong)]
@@ -348,6 +350,23 @@ class Solver:
                                                    _ptr(coeffs)))
         Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, norb, nw)
         return dict(G_cl=Gc, coeffs=coeffs.reshape(norb, 2, 4, maxnstep))
+
+    def green_real(self, iorb, ispin, maxnstep, omega, eta):
+        """G(w + i eta) of green_diag on real frequencies; A(w) = -Im G / pi."""
+        omega = _f64(omega)
+        g = np.zeros(2 * omega.size)
+        self._check(self._L.edzt_green_real(self._h, iorb, ispin, maxnstep, omega.size, _ptr(omega), float(eta),
+                                            _ptr(g)))
+        return g[0::2] + 1j * g[1::2]
+
+    def gs_occupancy(self, nspin=2):
+        """<n_{iorb,ispin}> [ispin][iorb] and double occupancies [iorb] of the
+        resident ground state (post_process.f90:62-112)."""
+        norb = self.model.norb
+        occ = np.zeros(norb * nspin)
+        docc = np.zeros(norb)
+        self._check(self._L.edzt_gs_occupancy(self._h, nspin, _ptr(occ), _ptr(docc)))
+        return occ.reshape(nspin, norb), docc
 
     def cluster_green_matrix(self, nspin, maxnstep, omega):
         """Full G_ab on the resident ground state (edzt_cluster_green_matrix),

@@ -875,7 +875,8 @@ void excitation(int nu, int nd, int pm, int ispin, int* ou, int* od)
 // Runs all requested excitation Lanczos runs, then the continued fractions.
 // g_out[r]: complex [nw] per run (host), ab_out[r]: host a (maxnstep) + b.
 void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, const double* omega_dev,
-                std::vector<std::vector<double>>& g_out, std::vector<std::vector<double>>& ab_out)
+                std::vector<std::vector<double>>& g_out, std::vector<std::vector<double>>& ab_out,
+                int real_axis = 0, double eta = 0.0)
 {
     const int nr = (int)runs.size();
     Lease<double> ab(c->pool, (size_t)std::max(nr, 1) * 2 * maxnstep);
@@ -956,7 +957,7 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
     if (!cj.empty()) {
         Lease<CFJob> dj(c->pool, cj.size());
         CK(cudaMemcpyAsync(dj.p, cj.data(), sizeof(CFJob) * cj.size(), cudaMemcpyHostToDevice, c->stream));
-        launch_cf(dj.p, (int)cj.size(), omega_dev, nw, c->stream);
+        launch_cf(dj.p, (int)cj.size(), omega_dev, nw, c->stream, real_axis, eta);
         g_launches += 1;
         CKLAUNCH();
         CK(cudaStreamSynchronize(c->stream));
@@ -1062,7 +1063,7 @@ void cluster_green_impl(edzt_ctx* c, int nspin, int maxnstep, int nw, const doub
 }
 
 void green_diag_impl(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, const double* omega, double* ap,
-                     double* bp, double* am, double* bm, double* g)
+                     double* bp, double* am, double* bm, double* g, int real_axis = 0, double eta = 0.0)
 {
     require_model(c);
     require_gs(c);
@@ -1076,7 +1077,7 @@ void green_diag_impl(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, con
     }
     InVec om(c, omega, nw);
     std::vector<std::vector<double>> gs, abs_;
-    green_runs(c, runs, maxnstep, nw, om.d, gs, abs_);
+    green_runs(c, runs, maxnstep, nw, om.d, gs, abs_, real_axis, eta);
     std::vector<double> gsum(2 * nw, 0.0);
     for (int r = 0; r < 2; r++)
         for (int q = 0; q < 2 * nw; q++) gsum[q] += gs[r][q];
@@ -1947,6 +1948,44 @@ int edzt_green_diag(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, cons
     return guarded(c, [&] {
         arg_check(ap && bp && am && bm && g && (omega || nw == 0), "bad arguments");
         green_diag_impl(c, iorb, ispin, maxnstep, nw, omega, ap, bp, am, bm, g);
+    });
+}
+
+int edzt_green_real(edzt_ctx* c, int iorb, int ispin, int maxnstep, int nw, const double* omega, double eta,
+                    double* g)
+{
+    return guarded(c, [&] {
+        arg_check(g != nullptr && (omega || nw == 0) && eta > 0.0, "bad arguments (eta > 0)");
+        green_diag_impl(c, iorb, ispin, maxnstep, nw, omega, nullptr, nullptr, nullptr, nullptr, g, 1, eta);
+    });
+}
+
+int edzt_gs_occupancy(edzt_ctx* c, int nspin, double* occ, double* docc)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        require_gs(c);
+        arg_check(nspin == 1 || nspin == 2, "nspin must be 1 or 2");
+        const int norb = c->mt.model.norb;
+        StrTable& su = str_table(c, c->gs_up);
+        StrTable& sd = str_table(c, c->gs_dn);
+        const long long dim = (long long)su.count * sd.count;
+        Lease<double> part(c->pool, (size_t)occ_partials_size());
+        launch_gs_occ(c->gs_vec.p, su.str->as<uint32_t>(), sd.str->as<uint32_t>(), su.count, dim, norb, part.p,
+                      c->stream);
+        g_launches += 1;
+        CKLAUNCH();
+        std::vector<double> hp((size_t)occ_partials_size());
+        CK(cudaMemcpyAsync(hp.data(), part.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        double sum[12] = {0.0};
+        for (size_t b = 0; b < hp.size() / 12; b++)
+            for (int q = 0; q < 12; q++) sum[q] += hp[b * 12 + q];
+        for (int ispin = 0; ispin < nspin; ispin++)
+            for (int a = 0; a < norb; a++)
+                if (occ) occ[a + norb * ispin] = sum[4 * ispin + a];
+        if (docc)
+            for (int a = 0; a < norb; a++) docc[a] = sum[8 + a];
     });
 }
 

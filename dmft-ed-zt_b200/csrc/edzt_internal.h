@@ -46,6 +46,11 @@ void launch_fill_start(double* v, long long n, uint64_t key, cudaStream_t s);
 void launch_copy(double* dst, const double* src, long long n, cudaStream_t s);
 
 void launch_apply_c(const ApplyCArgs& A, const double* in, double* out, cudaStream_t s);
+// Per-block partial sums [occ_partials_size()] = [block][12]: occupation of
+// orbital a by up (q = a), down (q = 4 + a) and both spins (q = 8 + a).
+int occ_partials_size();
+void launch_gs_occ(const double* x, const uint32_t* up, const uint32_t* dn, int nup, long long dim, int norb,
+                   double* part, cudaStream_t s);
 
 // Continued fractions (src/numeric_utils.f90:11-44) for many runs at once.
 struct CFJob {
@@ -57,7 +62,9 @@ struct CFJob {
     double sign;          // -1: z - a (continued_fraction_p), +1: z + a (continued_fraction_m)
     double* g;            // [nw] complex interleaved, written (levels >= 1)
 };
-void launch_cf(const CFJob* jobs_dev, int njobs, const double* omega, int nw, cudaStream_t s);
+// omega: Matsubara frequencies, or real frequencies with real_axis (z = w + i eta).
+void launch_cf(const CFJob* jobs_dev, int njobs, const double* omega, int nw, cudaStream_t s, int real_axis = 0,
+               double eta = 0.0);
 
 // ---- lanczos.cu: persistent fused Lanczos over a batch of jobs ------------
 enum LzMode { LZ_COEFF = 0, LZ_EIGVEC = 1 };

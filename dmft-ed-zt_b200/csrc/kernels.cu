@@ -225,7 +225,8 @@ __device__ __forceinline__ void cdiv_real(double num, double br, double bi, doub
     }
 }
 
-__global__ void k_cf(const CFJob* __restrict__ jobs, int njobs, const double* __restrict__ omega, int nw)
+__global__ void k_cf(const CFJob* __restrict__ jobs, int njobs, const double* __restrict__ omega, int nw,
+                     int real_axis, double eta)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= njobs * nw) return;
@@ -233,7 +234,8 @@ __global__ void k_cf(const CFJob* __restrict__ jobs, int njobs, const double* __
     const CFJob J = jobs[jb];
     const int n = J.levels;
     if (n < 1) return;
-    const double zr = J.zr_shift, zi = omega[iw];
+    // z = (+-E0) + i w_n on the Matsubara axis, (+-E0) + w + i eta on the real axis
+    const double zr = J.zr_shift + (real_axis ? omega[iw] : 0.0), zi = real_axis ? eta : omega[iw];
     auto bk = [&](int i) { return i == 0 ? J.b1 : J.b[i]; };   // b(1) = ||c^(+)|gs>|
     // the reference's recursion literally (numeric_utils.f90:18-22 / :39-43),
     // including its final level with b(1) when n == 1
@@ -246,9 +248,54 @@ __global__ void k_cf(const CFJob* __restrict__ jobs, int njobs, const double* __
     J.g[2 * iw + 1] = xi;
 }
 
-void launch_cf(const CFJob* jobs_dev, int njobs, const double* omega, int nw, cudaStream_t s)
+void launch_cf(const CFJob* jobs_dev, int njobs, const double* omega, int nw, cudaStream_t s, int real_axis,
+               double eta)
 {
     const int n = njobs * nw;
     if (n <= 0) return;
-    k_cf<<<(n + 127) / 128, 128, 0, s>>>(jobs_dev, njobs, omega, nw);
+    k_cf<<<(n + 127) / 128, 128, 0, s>>>(jobs_dev, njobs, omega, nw, real_axis, eta);
+}
+
+// ---------------------------------------------------------------------------
+// Occupancies of the ground state (post_process.f90:62-112):
+// occ(iorb, ispin) = sum |x_i|^2 over states with orbital iorb of spin ispin
+// filled, docc(iorb) = sum |x_i|^2 over states with both spins filled.
+// Fixed grid of per-block partial sums, summed in block order by the host.
+// ---------------------------------------------------------------------------
+static constexpr int kOccBlocks = 592;
+
+__global__ void __launch_bounds__(256) k_gs_occ(const double* __restrict__ x, const uint32_t* __restrict__ up,
+                                                const uint32_t* __restrict__ dn, int nup, long long dim, int norb,
+                                                double* __restrict__ part)
+{
+    __shared__ double scratch[12 * 32];
+    double acc[12];
+#pragma unroll
+    for (int q = 0; q < 12; q++) acc[q] = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += (long long)gridDim.x * blockDim.x) {
+        const long long id = i / nup;
+        const int iu = (int)(i - id * nup);
+        const double w = x[i] * x[i];
+        const uint32_t u = __ldg(up + iu), d = __ldg(dn + id);
+#pragma unroll
+        for (int a = 0; a < EDZT_MAX_NORB; a++) {
+            if (a < norb) {
+                const bool bu = (u >> a) & 1u, bd = (d >> a) & 1u;
+                acc[a] += bu ? w : 0.0;
+                acc[4 + a] += bd ? w : 0.0;
+                acc[8 + a] += (bu && bd) ? w : 0.0;
+            }
+        }
+    }
+    block_sum<12>(acc, scratch);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 12; q++) part[(size_t)blockIdx.x * 12 + q] = acc[q];
+}
+
+int occ_partials_size() { return kOccBlocks * 12; }
+
+void launch_gs_occ(const double* x, const uint32_t* up, const uint32_t* dn, int nup, long long dim, int norb,
+                   double* part, cudaStream_t s)
+{
+    k_gs_occ<<<kOccBlocks, 256, 0, s>>>(x, up, dn, nup, dim, norb, part);
 }

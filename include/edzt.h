@@ -155,6 +155,18 @@ int edzt_green_diag(edzt_ctx *ctx, int iorb, int ispin, int maxnstep, int nw, co
 int edzt_cluster_green_ftn(edzt_ctx *ctx, int nspin, int maxnstep, int nw, const double *omega,
                            double *G_cl, double *coeffs);
 
+/* green_diag on the real axis: g(w) = CF_p(E0 + w + i eta) + CF_m(-E0 + w +
+ * i eta) at the real frequencies omega[nw] (complex [nw]); the spectral
+ * function is A(w) = -Im g(w) / pi (utils/spectral_ftn.py:35-44, which passes
+ * the c^+ coefficients to CF_m as well; here each fraction gets its own). */
+int edzt_green_real(edzt_ctx *ctx, int iorb, int ispin, int maxnstep, int nw, const double *omega, double eta,
+                    double *g);
+
+/* Occupancies of the resident ground state (src/post_process.f90:62-112):
+ * occ(norb, nspin) (column-major, nullable) = <n_{iorb,ispin}>, docc(norb)
+ * (nullable) = <n_{iorb,up} n_{iorb,down}>, summed on the device. */
+int edzt_gs_occupancy(edzt_ctx *ctx, int nspin, double *occ, double *docc);
+
 /* Full cluster Green's function matrix on the resident ground state:
  * G(nw, norb, norb, nspin) complex (column-major, interleaved).  No
  * counterpart in the reference, which computes the diagonal only

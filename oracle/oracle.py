@@ -267,6 +267,25 @@ class Oracle:
         Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, self.norb, nw)   # (ispin, iorb, iw)
         return dict(G_cl=Gc, coeffs=coeffs.reshape(self.norb, 2, 4, maxnstep))
 
+    def occupancy(self, ne_up, ne_dn, gsvec, nspin):
+        """occ[ispin][iorb] and docc[iorb] of a ground state
+        (post_process.f90:62-112): |x_i|^2 summed over the states whose
+        orbital bit is set (both spins for docc)."""
+        up, dn = self.basis(ne_up, ne_dn)
+        up = np.asarray(up, dtype=np.int64)
+        dn = np.asarray(dn, dtype=np.int64)
+        w = (np.asarray(gsvec, dtype=np.float64) ** 2).reshape(len(dn), len(up))
+        occ = np.zeros((nspin, self.norb))
+        docc = np.zeros(self.norb)
+        for a in range(self.norb):
+            bu = ((up >> a) & 1).astype(bool)
+            bd = ((dn >> a) & 1).astype(bool)
+            occ[0, a] = w[:, bu].sum()
+            if nspin == 2:
+                occ[1, a] = w[bd, :].sum()
+            docc[a] = w[np.ix_(bd, bu)].sum()
+        return occ, docc
+
     def green_run(self, v_init, nu, nd, pm, e0, maxnstep, omega):
         """One c^+ (pm=1) or c (pm=2) run of green_diag (dmft_green.f90:204-257)
         from an explicit start vector in sector (nu, nd): Lanczos, b(1) =

@@ -208,3 +208,50 @@ def test_cluster_green_matrix_coupled_orbitals(pkg, solver, oracle_mod):
     G = solver.cluster_green_matrix(2, 150, omega)
     assert np.abs(G - ref).max() <= G_TOL
     assert np.abs(G[:, 0, 1]).max() > 1e-3
+
+
+def test_gs_occupancy(solver, configs, oracle_mod):
+    """<n_{a,s}> and <n_{a,up} n_{a,down}> of the ground state on the device
+    (post_process.f90:62-112) against the oracle's sums."""
+    for cfg, seed in ((configs.kanamori_n10(), 1), (configs.bethe_n6(), 7)):
+        o = oracle_for(oracle_mod, cfg["model"])
+        gs_ref = o.ground_state(cfg["sectors"], cfg["maxnstep"], seed=seed)
+        occ_ref, docc_ref = o.occupancy(*gs_ref["sector"], gs_ref["vec"], 2)
+        solver.set_model(cfg["model"])
+        gs = solver.ground_state(cfg["sectors"], cfg["maxnstep"], seed=seed)
+        occ, docc = solver.gs_occupancy(2)
+        assert np.abs(occ - occ_ref).max() <= 1e-10 and np.abs(docc - docc_ref).max() <= 1e-10
+        nu, nd = gs["sector"]
+        norb = cfg["model"].norb
+        assert occ[0].sum() <= nu + 1e-12 and occ[1].sum() <= nd + 1e-12
+        assert np.all(docc <= np.minimum(occ[0], occ[1]) + 1e-12)
+
+
+def test_green_real_axis_and_sum_rule(solver, configs, oracle_mod):
+    """green_diag on the real axis (the spectral function of
+    utils/spectral_ftn.py with each fraction on its own coefficients)
+    against the oracle's coefficients evaluated at w + i eta; A(w) carries the
+    total weight <c c^+> + <c^+ c> = 1 up to the Lorentzian tails."""
+    cfg = configs.bethe_n6()
+    o = oracle_for(oracle_mod, cfg["model"])
+    gs_ref = o.ground_state(cfg["sectors"], cfg["maxnstep"], seed=7)
+    w = np.linspace(-8.0, 8.0, 4001)
+    eta = 0.05
+    ref = o.green_diag(*gs_ref["sector"], gs_ref["vec"], gs_ref["e0"], 1, 1, cfg["maxnstep"],
+                       oracle_mod.matsubara(4, cfg["beta"]))
+    e0 = gs_ref["e0"]
+    np_, nm_ = ref["nstep"]
+    lev = lambda n: 2 if (n == 1 and cfg["maxnstep"] >= 2) else n
+    g_ref = np.array([oracle_mod.continued_fraction(complex(e0 + x, eta), lev(np_), ref["ap"], ref["bp"], -1)
+                      + oracle_mod.continued_fraction(complex(-e0 + x, eta), lev(nm_), ref["am"], ref["bm"], +1)
+                      for x in w])
+    solver.set_model(cfg["model"])
+    solver.ground_state(cfg["sectors"], cfg["maxnstep"], seed=7)
+    g = solver.green_real(1, 1, cfg["maxnstep"], w, eta)
+    # near a pole G(w + i eta) is of order 1/eta: rounding-level differences
+    # of the higher Lanczos levels (the two implementations agree to 1e-8 on
+    # the Matsubara axis) show up amplified, hence 1e-6 of max |G| here
+    assert np.abs(g - g_ref).max() <= 1e-6 * np.abs(g_ref).max()
+    A = -g.imag / np.pi
+    assert np.all(A >= -1e-12)
+    assert abs(np.trapezoid(A, w) - 1.0) < 0.02
