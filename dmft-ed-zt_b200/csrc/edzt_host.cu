@@ -558,7 +558,6 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     unsigned* d_sw = reinterpret_cast<unsigned*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part));
     std::vector<unsigned> sw(bytes_sw / sizeof(unsigned), 0u);
     sw[64] = (unsigned)nj;   // runs still going
-    sw[96] = (unsigned)nj;   // its snapshot at the last barrier
     CK(cudaMemcpyAsync(d_jobs, jobs.data(), bytes_jobs, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(d_st, st.data(), bytes_st, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(d_pre, prefix.data(), bytes_pre, cudaMemcpyHostToDevice, c->stream));

@@ -46,11 +46,12 @@ static constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000ull * 1000ull
 static constexpr int kFixedDoubles = 128 + EDZT_MAX_P * EDZT_MAX_P + EDZT_MAX_AMP;   // reduction scratch, wint, amp
 static constexpr int kBarGroup = 16;                                  // CTAs per barrier group
 
-// sync words (unsigned), each counter on its own 128-byte line
+// sync words (unsigned), each counter on its own 128-byte line; SW_GEN is a
+// 64-bit word (barrier count << 32 | runs still going)
 #define SW_GEN 0
 #define SW_TOP 32
 #define SW_ACTIVE 64
-#define SW_SNAP 96
+
 #define SW_GROUP(g) (128 + 32 * (g))
 
 size_t lz_sync_bytes(int G) { return sizeof(unsigned) * (128 + 32 * (size_t)((G + kBarGroup - 1) / kBarGroup)); }
@@ -89,37 +90,53 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     return t;
 }
 
-// Hierarchical grid barrier with a bounded wait: CTAs arrive on a counter of
-// their group of 16, the last of each group on the top counter, the last of
-// all snapshots the active-run counter and releases.  Returns false (and the
-// kernel stops) when the wait ran out or another CTA reported an error.
-__device__ bool grid_barrier(unsigned* sw, int* status)
+// Hierarchical grid barrier with a bounded wait.  Counters only grow: the
+// k-th barrier of a launch is complete on a group counter at k * (group
+// size) arrivals and on the top counter at k * (number of groups), so no
+// counter is read before arriving or reset after.  CTAs arrive on the counter
+// of their group of 16, the last of each group on the top counter, and the
+// last of all publishes (k << 32 | runs still going) in the 64-bit
+// generation word, which the others wait for.  Returns false (and the kernel
+// stops) when the wait ran out or another CTA reported an error; *snap
+// receives the number of runs still going.
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ bool grid_barrier(unsigned* sw, int* status, unsigned& nbar, unsigned& snap)
 {
     __shared__ int s_ok;
+    __shared__ unsigned s_snap;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned gen = ld_acquire_u32(sw + SW_GEN);
+        const unsigned k1 = nbar + 1u;
         const int G = gridDim.x;
         const int g = blockIdx.x / kBarGroup;
-        const int ngroups = (G + kBarGroup - 1) / kBarGroup;
+        const unsigned ngroups = (unsigned)((G + kBarGroup - 1) / kBarGroup);
         const unsigned gsize = (unsigned)min(kBarGroup, G - g * kBarGroup);
-        __threadfence();
+        unsigned long long* genw = reinterpret_cast<unsigned long long*>(sw + SW_GEN);
+        __threadfence();                                  // this CTA's sums and states before its arrival
         bool last = false;
-        if (atomicAdd(sw + SW_GROUP(g), 1u) == gsize - 1u) {
-            atomicExch(sw + SW_GROUP(g), 0u);
-            __threadfence();
-            last = atomicAdd(sw + SW_TOP, 1u) == (unsigned)ngroups - 1u;
-        }
+        if (atomicAdd(sw + SW_GROUP(g), 1u) == k1 * gsize - 1u)
+            last = atomicAdd(sw + SW_TOP, 1u) == k1 * ngroups - 1u;
+        unsigned long long w;
         if (last) {
-            atomicExch(sw + SW_TOP, 0u);
-            atomicExch(sw + SW_SNAP, atomicAdd(sw + SW_ACTIVE, 0u));
-            __threadfence();
-            atomicAdd(sw + SW_GEN, 1u);
+            const unsigned act = atomicAdd(sw + SW_ACTIVE, 0u);   // every arrival's decrements are in
+            w = ((unsigned long long)k1 << 32) | act;
+            st_release_u64(genw, w);
         } else {
             const unsigned long long t0 = globaltimer_ns();
             unsigned it = 0;
-            while (ld_acquire_u32(sw + SW_GEN) == gen) {
+            while ((unsigned)((w = ld_acquire_u64(genw)) >> 32) < k1) {
                 if (ld_acquire_s32(status) != EDZT_DEV_OK) { ok = 0; break; }
                 if ((++it & 255u) == 0u && globaltimer_ns() - t0 > kBarrierTimeoutNs) {
                     atomicCAS(status, EDZT_DEV_OK, EDZT_DEV_BARRIER_TIMEOUT);
@@ -130,9 +147,12 @@ __device__ bool grid_barrier(unsigned* sw, int* status)
             }
         }
         __threadfence();
+        s_snap = (unsigned)w;
         s_ok = ok && (ld_acquire_s32(status) == EDZT_DEV_OK);
     }
     __syncthreads();
+    nbar++;
+    snap = s_snap;
     return s_ok != 0;
 }
 
@@ -231,9 +251,10 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
     double* chunk_base = smem + kFixedDoubles;           // staged rows of the current tile
     __shared__ LzJob sJ;
     __shared__ LzState sS;
-    __shared__ int s_job, s_run;
+    __shared__ int s_job;
 
     const int G = gridDim.x;
+    unsigned nbar = 0u;                                  // grid barriers this CTA has passed
     if (threadIdx.x == 0) s_job = -1;
     __syncthreads();
 
@@ -277,10 +298,7 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
             const bool first = (my_q() == 0);
             Sums s{v[0], v[1], v[2], v[3]};
             sS = advance(sJ, prev, s, first, sw);
-            if (first) {
-                state[2 * (size_t)j + (pass & 1)] = sS;
-                __threadfence();
-            }
+            if (first) state[2 * (size_t)j + (pass & 1)] = sS;   // published by the barrier's fence
         }
         __syncthreads();
     };
@@ -458,10 +476,9 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
             else step_tile(std::false_type{}, tl, acc);
         }
         if (cur >= 0 && sS.active) flush(pass, acc);
-        if (!grid_barrier(sw, status)) return;
-        if (threadIdx.x == 0) s_run = ld_acquire_u32(sw + SW_SNAP) > 0u;
-        __syncthreads();
-        if (!s_run) break;
+        unsigned running = 0u;
+        if (!grid_barrier(sw, status, nbar, running)) return;
+        if (running == 0u) break;
     }
 }
 
