@@ -20,6 +20,8 @@ and seeded: the reference quotes no data set.
              this host's cores, on a bounded sample of the workload
   plain_gpu  the reference's Lanczos structure run kernel by kernel on the
              same GPU (the one-solve-at-a-time drop-in comparator)
+  hv         standalone H.v (edzt_hx) at nsite 12/14/16: GB/s at 16 B per
+             state against the measured HBM peak
   batched    the batched form (one GPU): the first --batched instances of the
              seeded 256-instance draw (nsite ~ U{8..14}) in one
              edzt_solve_batch call, solves/s, with the plain engine's solves/s
@@ -233,6 +235,41 @@ def served_leg(pkg, s, cfgs, n, seed=5):
                       "each and do not fit the bench's time bound), Poisson 200/s (seed 5)"}
 
 
+def hv_leg(pkg, s, peak):
+    """Standalone H.v (edzt_hx, y = H x) on the half-filled sector of a
+    single-orbital impurity at nsite 12, 14, 16: device time per H.v (CUDA
+    events on the library's stream, median of 5 after 2 warm-up), achieved
+    GB/s at 16 B per state (x read, y written) against the measured peak."""
+    import numpy as np
+    import torch
+    stream = torch.cuda.ExternalStream(s.stream_ptr(), device=torch.device("cuda", torch.cuda.current_device()))
+    out = {}
+    for ns in (12, 14, 16):
+        nb = ns - 1
+        rng = np.random.default_rng(ns)
+        m = pkg.Model(1, nb, np.zeros((1, 2)), np.stack([rng.uniform(-2, 2, nb)] * 2, 1),
+                      np.stack([rng.uniform(0.1, 1, nb)] * 2, 1).reshape(1, nb, 2), U=3.0, mu=1.5)
+        s.set_model(m)
+        n = s.dim(ns // 2, ns // 2)
+        x = torch.rand(n, dtype=torch.float64, device="cuda")
+        y = torch.empty_like(x)
+        ts = []
+        for it in range(7):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.hx(ns // 2, ns // 2, x, y)
+            e1.record(stream)
+            e1.synchronize()
+            if it >= 2:
+                ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        gbs = 16.0 * n / (ms / 1000.0) / 1e9
+        out[f"nsite{ns}"] = {"dim": int(n), "ms": ms, "achieved_GBs": gbs, "frac": gbs / peak if peak else None}
+        del x, y
+    return out
+
+
 def read_traffic(path):
     """DRAM bytes per k_lanczos launch (dram__bytes_read.sum + dram__bytes_write.sum
     from one ncu capture of this workload), from the `bytes_per_launch:` line of
@@ -440,6 +477,7 @@ def run_gpu(args):
                         "and Green's-function launches (<= 27 MB) are L2-resident"}
     roofline["traffic"] = read_traffic(args.traffic_file)
 
+    hv = hv_leg(pkg, s, peak) if (world == 1 and not args.skip_hv) else None
     batched = served = None
     if world == 1 and args.batched > 0:
         cfgs = importlib.import_module("dmft_ed_zt_b200.configs")
@@ -462,7 +500,7 @@ def run_gpu(args):
                 "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)),
                                "p99": float(np.percentile(lat_sorted, 99))},
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
-                "plain_gpu": plain, "batched": batched, "served": served, "clocks": clk, "e0": e0.value}
+                "plain_gpu": plain, "hv": hv, "batched": batched, "served": served, "clocks": clk, "e0": e0.value}
         print(json.dumps(line))
     s.close()
     if dist is not None:
@@ -479,6 +517,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-hv", action="store_true")
     ap.add_argument("--batched", type=int, default=64, help="instances of the batched leg (0: skip)")
     ap.add_argument("--served", type=int, default=32, help="requests of the served leg (0: skip)")
     ap.add_argument("--traffic-file", default=os.path.join(ROOT, "profiles", "k_lanczos_aim_n12_dram.txt"))

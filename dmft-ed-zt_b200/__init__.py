@@ -50,6 +50,7 @@ EXPORTS = (
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
     "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
     "edzt_cluster_green_matrix", "edzt_gs_occupancy", "edzt_green_real", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
+    "edzt_server_cancel", "edzt_instance_footprint", "edzt_set_fault_test",
 )
 # Limits of edzt_lanczos_iteration_noalloc (its static scratch array).
 NOALLOC_MAX_DIM = 262144
@@ -129,6 +130,9 @@ def load_library(path: str = LIB_PATH):
     L.edzt_server_result.argtypes = [_vp, C.c_longlong, _ip, _ip, _dp, _vp]
     L.edzt_server_destroy.argtypes = [_vp]
     L.edzt_server_destroy.restype = None
+    L.edzt_server_cancel.argtypes = [_vp, C.c_longlong]
+    L.edzt_instance_footprint.argtypes = [_vp, C.POINTER(C.c_longlong)]
+    L.edzt_set_fault_test.argtypes = [_vp, C.c_int, C.c_double, C.c_int]
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
     L.edzt_ground_state.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_uint64, _ip, _dp, _vp, _vp]
     L.edzt_gs_dim.argtypes = [_vp]
@@ -379,6 +383,19 @@ class Solver:
         Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, norb, norb, nw)   # [s, b, a, iw]
         return Gc.transpose(0, 2, 1, 3)
 
+    def set_fault_test(self, pass_cap=0, wait_seconds=0.0, stall_cta=-1):
+        """Fault tests of the persistent kernel (edzt_set_fault_test); all
+        defaults restore normal operation."""
+        self._check(self._L.edzt_set_fault_test(self._h, int(pass_cap), float(wait_seconds), int(stall_cta)))
+
+    def footprint(self, inst) -> int:
+        """Device bytes a request holds at its peak (edzt_instance_footprint)."""
+        keep = []
+        rec = _instance(inst, keep)
+        b = C.c_longlong()
+        self._check(self._L.edzt_instance_footprint(C.byref(rec), C.byref(b)))
+        return b.value
+
     def solve_batch(self, instances, maxnstep, omega, hbm_budget=0):
         """Many independent solves in batched persistent launches
         (edzt_solve_batch).  instances: dicts with model, sectors, nspin (1),
@@ -459,6 +476,9 @@ class Server:
             return None
         del self._shape[rid]
         return dict(isector=isec.value, e0=e0.value, G_cl=(G[0::2] + 1j * G[1::2]).reshape(nspin, norb, self.nw))
+
+    def cancel(self, rid: int):
+        self.solver._check(self._L.edzt_server_cancel(self._h, rid))
 
     def close(self):
         if self._h:

@@ -203,6 +203,10 @@ struct edzt_ctx {
     std::unique_ptr<DevBuf> scal;          // device scalars
     std::unique_ptr<DevBuf> dot_part;      // dot partials
     long long launches_at_create = 0;
+    // fault-test settings (edzt_set_fault_test): pass cap, barrier wait limit, stalled CTA
+    int dbg_pass_cap = 0;
+    unsigned long long dbg_wait_ns = 0;
+    int dbg_stall_cta = -1;
 };
 
 namespace {
@@ -386,6 +390,14 @@ DevModel model_from(int norb, int nbath, const double* em, const double* ek, con
             for (int l = 0; l < nbath; l++) m.vmk[a][l][s] = vmk[a + norb * (l + nbath * s)];
     }
     m.U = U; m.Up = Up; m.Jex = Jex; m.Jp = Jp; m.mu = mu;
+    bool finite = std::isfinite(U) && std::isfinite(Up) && std::isfinite(Jex) && std::isfinite(Jp) && std::isfinite(mu);
+    for (int s = 0; s < 2; s++) {
+        for (int a = 0; a < norb; a++) finite = finite && std::isfinite(m.em[a][s]);
+        for (int l = 0; l < nbath; l++) finite = finite && std::isfinite(m.ek[l][s]);
+        for (int a = 0; a < norb; a++)
+            for (int l = 0; l < nbath; l++) finite = finite && std::isfinite(m.vmk[a][l][s]);
+    }
+    arg_check(finite, "model parameters must be finite");
     return m;
 }
 
@@ -571,6 +583,9 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     B.smem = smem;
     B.total_tiles = prefix[nj];
     B.max_passes = 2 * max_steps + 4;   // start vector, every step, and room for repeated steps
+    if (c->dbg_pass_cap > 0) B.max_passes = std::min(B.max_passes, c->dbg_pass_cap);
+    B.wait_ns = c->dbg_wait_ns;
+    B.stall_cta = c->dbg_stall_cta;
     CK(cudaEventRecord(c->ev0, c->stream));
     CK(launch_lanczos_persistent(B, d_jobs, d_st, d_pre, d_part, d_sw, c->status->as<int>(), c->stream));
     CK(cudaEventRecord(c->ev1, c->stream));
@@ -1394,6 +1409,7 @@ struct ServReq {
     long long id = 0;
     BatchInst I;
     int phase = 0;                         // 1 scan, 2 eigenvector, 3 Green's runs, 4 done
+    bool cancelled = false;
     Lease<double> ab;                      // [nsector][2][maxnstep] scan coefficients (device)
     std::vector<int> job_of_sector;        // scan job of each sector in the current launch, -1 if none
     std::vector<double> hab;               // scan coefficients on the host
@@ -1444,6 +1460,8 @@ int server_step(edzt_server* sv)
     const int maxnstep = sv->maxnstep, nw = sv->nw;
     server_admit(sv);
     std::vector<JobSpec> specs;
+    for (auto& up : sv->active)                               // cancelled requests leave now
+        if (up->cancelled) { up->error = "cancelled"; up->phase = 4; }
     for (auto& up : sv->active) {
         ServReq& q = *up;
         BatchInst& I = q.I;
@@ -1501,8 +1519,7 @@ int server_step(edzt_server* sv)
             }
         }
     }
-    if (specs.empty()) return 0;
-    run_jobs(c, specs);
+    if (!specs.empty()) run_jobs(c, specs);
 
     // after the launch: every request moves one phase on
     std::vector<ServReq*> scan, eig, green;
@@ -2035,6 +2052,10 @@ int edzt_server_submit(edzt_server* sv, const edzt_instance* inst, long long* id
         arg_check(inst != nullptr && id != nullptr, "inst and id required");
         auto q = std::make_unique<ServReq>();
         init_inst(*inst, q->I);
+        if (q->I.footprint > sv->budget)
+            throw EdztError{EDZT_ERR_OOM, "request needs " + std::to_string(q->I.footprint) +
+                                              " bytes of device memory, the server's budget is " +
+                                              std::to_string(sv->budget)};
         q->id = sv->next_id++;
         *id = q->id;
         sv->queue.push_back(std::move(q));
@@ -2072,6 +2093,47 @@ int edzt_server_result(edzt_server* sv, long long id, int* done, int* isector, d
         if (G_cl && !q.G.empty()) copy_out(sv->c, G_cl, q.G.data(), sizeof(double) * q.G.size());
         CK(cudaStreamSynchronize(sv->c->stream));
         sv->finished.erase(it);
+    });
+}
+
+int edzt_server_cancel(edzt_server* sv, long long id)
+{
+    if (!sv) return EDZT_ERR_ARG;
+    return guarded(sv->c, [&] {
+        for (auto it = sv->queue.begin(); it != sv->queue.end(); ++it)
+            if ((*it)->id == id) {
+                sv->queue.erase(it);
+                return;
+            }
+        for (auto& q : sv->active)
+            if (q->id == id) {
+                q->cancelled = true;   // retired, its memory released, at the next step
+                return;
+            }
+        throw EdztError{EDZT_ERR_ARG, "no queued or running request " + std::to_string(id)};
+    });
+}
+
+int edzt_instance_footprint(const edzt_instance* inst, long long* bytes)
+{
+    if (!inst || !bytes) return EDZT_ERR_ARG;
+    try {
+        BatchInst I;
+        init_inst(*inst, I);
+        *bytes = I.footprint;
+        return EDZT_OK;
+    } catch (const EdztError& e) {
+        return e.code;
+    }
+}
+
+int edzt_set_fault_test(edzt_ctx* c, int pass_cap, double wait_seconds, int stall_cta)
+{
+    return guarded(c, [&] {
+        arg_check(pass_cap >= 0 && wait_seconds >= 0.0 && stall_cta >= -1, "bad fault-test settings");
+        c->dbg_pass_cap = pass_cap;
+        c->dbg_wait_ns = (unsigned long long)(wait_seconds * 1e9);
+        c->dbg_stall_cta = stall_cta;
     });
 }
 

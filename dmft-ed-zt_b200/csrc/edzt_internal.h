@@ -112,6 +112,8 @@ struct LzBatch {
     int max_passes;
     size_t smem;
     long long total_tiles;
+    unsigned long long wait_ns;   // grid-barrier wait limit (0: the default 5 s)
+    int stall_cta;                // fault test: this CTA leaves without arriving (-1: none)
 };
 
 int lz_grid_size(int device, size_t smem, int* block_out);

@@ -111,8 +111,10 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ bool grid_barrier(unsigned* sw, int* status, unsigned& nbar, unsigned& snap)
+__device__ bool grid_barrier(unsigned* sw, int* status, unsigned& nbar, unsigned& snap, const LzBatch& B)
 {
+    if ((int)blockIdx.x == B.stall_cta) return false;   // fault test: leave without arriving
+    const unsigned long long limit = B.wait_ns ? B.wait_ns : kBarrierTimeoutNs;
     __shared__ int s_ok;
     __shared__ unsigned s_snap;
     __syncthreads();
@@ -138,7 +140,7 @@ __device__ bool grid_barrier(unsigned* sw, int* status, unsigned& nbar, unsigned
             unsigned it = 0;
             while ((unsigned)((w = ld_acquire_u64(genw)) >> 32) < k1) {
                 if (ld_acquire_s32(status) != EDZT_DEV_OK) { ok = 0; break; }
-                if ((++it & 255u) == 0u && globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+                if ((++it & 255u) == 0u && globaltimer_ns() - t0 > limit) {
                     atomicCAS(status, EDZT_DEV_OK, EDZT_DEV_BARRIER_TIMEOUT);
                     ok = 0;
                     break;
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
         }
         if (cur >= 0 && sS.active) flush(pass, acc);
         unsigned running = 0u;
-        if (!grid_barrier(sw, status, nbar, running)) return;
+        if (!grid_barrier(sw, status, nbar, running, B)) return;
         if (running == 0u) break;
     }
 }

@@ -178,6 +178,7 @@ void run(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, 
     B.smem = smem;
     B.total_tiles = J.ntiles;
     B.max_passes = 2 * maxnstep + 4;
+    B.stall_cta = -1;
     NA_CK(launch_lanczos_persistent(B, d_job, d_state, d_prefix, d_part, d_sync, d_status, st));
     edzt_count_launches(1);
     int status = 0;

@@ -229,7 +229,25 @@ int edzt_server_step(edzt_server *srv, int *nactive, int *nqueued, int *nfinishe
  * nullable) once request id has finished, which also releases it; *done = 0
  * while it runs. */
 int edzt_server_result(edzt_server *srv, long long id, int *done, int *isector, double *e0, double *G_cl);
+/* Removes a queued request, or marks a running one to leave at the next step
+ * (its memory is released then); its result call reports EDZT_ERR_NUMERIC
+ * "cancelled".  edzt_server_submit rejects a request whose device-memory
+ * footprint exceeds the server's budget with EDZT_ERR_OOM. */
+int edzt_server_cancel(edzt_server *srv, long long id);
 void edzt_server_destroy(edzt_server *srv);
+/* Device-memory footprint (bytes) a request holds at its peak in the batched
+ * and served forms: the sector scan's pair buffers (32 B per state of every
+ * sector) or its Green's runs', whichever is larger, plus its ground state. */
+int edzt_instance_footprint(const edzt_instance *inst, long long *bytes);
+
+/* Fault tests (no counterpart in the reference; no GPU fault is involved):
+ * pass_cap > 0 caps the passes of a persistent launch (a run that needs more
+ * fails with EDZT_ERR_NUMERIC); wait_seconds > 0 shortens the grid-barrier
+ * wait limit (default 5 s); stall_cta >= 0 makes that CTA leave the launch
+ * without arriving at the next grid barrier, so the others' bounded wait runs
+ * out and the call returns EDZT_ERR_TIMEOUT.  All zero / -1: normal
+ * operation.  The context stays usable after either error. */
+int edzt_set_fault_test(edzt_ctx *ctx, int pass_cap, double wait_seconds, int stall_cta);
 
 /* Kernel launches issued by this context since creation (instrumentation). */
 long long edzt_launch_count(const edzt_ctx *ctx);

@@ -71,10 +71,13 @@ def test_server_mix_equals_alone(pkg, solver, configs):
 
 
 def test_server_budget_admits_one_at_a_time(pkg, solver, configs):
-    reqs = _requests(pkg, configs, n=3, seed=32)
+    rng = np.random.default_rng(32)
+    reqs = [dict(model=random_model(pkg, rng, 1, 7), sectors=configs.near_half_sectors(8), nspin=1,
+                 seed=int(rng.integers(1 << 40))) for _ in range(3)]                   # equal footprints
     omega = pkg.matsubara(64, 30.0)
     ref = _alone(solver, reqs, omega, 80)
-    sv = pkg.Server(solver, 80, omega, hbm_budget=1)
+    budget = int(1.5 * max(solver.footprint(r) for r in reqs))                      # one fits at a time
+    sv = pkg.Server(solver, 80, omega, hbm_budget=budget)
     try:
         ids = [sv.submit(r) for r in reqs]
         na, nq, nf = sv.step()
