@@ -9,6 +9,7 @@ of the reference (yw-choi/DMFT-ED-ZT) that the library replaces:
   apply_c             src/ed_operator.f90:13-57
   lanczos_iteration   src/lanczos_solver.f90:92-173
   diag_lanczos        src/lanczos_solver.f90:20-90
+  diag_arpack         src/arpack_solver.f90:19-124
   ground_state        src/ground_state.f90:1-81
   green_diag          src/dmft_green.f90:177-260
   cluster_green_ftn   src/dmft_green.f90:47-126
@@ -50,8 +51,12 @@ EXPORTS = (
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
     "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
     "edzt_cluster_green_matrix", "edzt_gs_occupancy", "edzt_green_real", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
-    "edzt_server_cancel", "edzt_instance_footprint", "edzt_set_fault_test",
+    "edzt_server_cancel", "edzt_instance_footprint", "edzt_set_fault_test", "edzt_diag_arpack",
+    "edzt_set_diag_solver",
 )
+# ground_state's diag_solver values (src/ground_state.f90:53-60).
+DIAG_LANCZOS = 1
+DIAG_ARPACK = 2
 # Limits of edzt_lanczos_iteration_noalloc (its static scratch array).
 NOALLOC_MAX_DIM = 262144
 NOALLOC_MAX_STEPS = 2048
@@ -134,6 +139,8 @@ def load_library(path: str = LIB_PATH):
     L.edzt_instance_footprint.argtypes = [_vp, C.POINTER(C.c_longlong)]
     L.edzt_set_fault_test.argtypes = [_vp, C.c_int, C.c_double, C.c_int]
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
+    L.edzt_diag_arpack.argtypes = [_vp, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _vp, _vp, _ip]
+    L.edzt_set_diag_solver.argtypes = [_vp, C.c_int]
     L.edzt_ground_state.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_uint64, _ip, _dp, _vp, _vp]
     L.edzt_gs_dim.argtypes = [_vp]
     L.edzt_gs_dim.restype = C.c_longlong
@@ -320,6 +327,22 @@ class Solver:
         self._check(self._L.edzt_diag_lanczos(self._h, ne_up, ne_dn, maxnstep, C.c_uint64(seed),
                                               C.c_uint64(stream), C.byref(ev), _ptr(vec), C.byref(res)))
         return dict(e0=ev.value, vec=vec, residual=res.value)
+
+    def diag_arpack(self, ne_up, ne_dn, seed=0, stream=0, want_resid=True):
+        """diag_arpack (src/arpack_solver.f90:19-124): the lowest eigenpair by
+        the restarted Lanczos with ARPACK's settings (nev 3, ncv 6, 'SA', tol 0)."""
+        ev = C.c_double()
+        nmult = C.c_int()
+        vec = np.zeros(self.dim(ne_up, ne_dn))
+        ritz = np.zeros(3)
+        resid = np.zeros(3) if want_resid else None
+        self._check(self._L.edzt_diag_arpack(self._h, ne_up, ne_dn, C.c_uint64(seed), C.c_uint64(stream),
+                                             C.byref(ev), _ptr(vec), _ptr(ritz), _ptr(resid), C.byref(nmult)))
+        return dict(e0=ev.value, vec=vec, ritz=ritz, resid=resid, nmult=nmult.value)
+
+    def set_diag_solver(self, diag_solver: int):
+        """ground_state's diag_solver: DIAG_LANCZOS (1) or DIAG_ARPACK (2)."""
+        self._check(self._L.edzt_set_diag_solver(self._h, int(diag_solver)))
 
     def ground_state(self, sectors, maxnstep, seed=0, want_vec=True):
         sec = np.ascontiguousarray(np.asarray(sectors, dtype=np.int32).reshape(-1, 2))

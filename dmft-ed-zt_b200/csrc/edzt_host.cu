@@ -182,6 +182,7 @@ struct edzt_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     int engine = EDZT_ENGINE_FUSED;
+    int diag_solver = EDZT_DIAG_LANCZOS;    // ground_state's diag_solver (ground_state.f90:53-60)
     ModelTables mt;                         // the model of the single-model entry points
     // bit strings and rank tables by (nsite, electron count): model-independent, shared
     std::map<std::pair<int, int>, std::unique_ptr<StrTable>> str_tables;
@@ -709,12 +710,232 @@ double finish_eigvec(edzt_ctx* c, const DevSector& S, double* vec, double e0)
     return plain_dot(c, v.p, v.p, n);
 }
 
+// ---------------------------------------------------------------------------
+// diag_arpack (src/arpack_solver.f90:19-124): the lowest eigenpair of a sector
+// by a restarted Lanczos with the reference's ARPACK settings: nev = 3 wanted
+// eigenvalues, which = 'SA' (smallest algebraic), ncv = 6 basis vectors,
+// tol = 0 (machine precision), exact shifts, at most 20000 restarts.
+//
+// ARPACK's implicit restart with exact shifts keeps the span of the wanted
+// Ritz vectors and the residual.  The thick restart (K. Wu and H. Simon,
+// SIAM J. Matrix Anal. Appl. 22 (2000) 602-616) keeps that span explicitly:
+// the kept Ritz vectors, then the normalised residual, with the projected
+// matrix an arrow (Ritz values on the diagonal, beta_m * y_{m,i} on the
+// border) that the next Lanczos steps extend.  Convergence is ARPACK's test
+// (dsconv): Ritz estimate |beta_m y_{m,i}| <= tol * max(eps^(2/3), |theta_i|)
+// for all nev wanted values, tol = eps = 2^-53.  The number kept grows with
+// the converged count as in dsaup2: nev + min(nconv, (ncv - nev) / 2).
+// Every new vector is orthogonalised against the whole basis twice.
+// ---------------------------------------------------------------------------
+constexpr int kArNev = 3, kArNcv = 6, kArMaxItr = 20000;
+
+struct ArpackOut {
+    double eigval = 0.0;
+    double ritz[kArNev] = {0, 0, 0}, bounds[kArNev] = {0, 0, 0}, resid[kArNev] = {0, 0, 0};
+    int nmult = 0, nrestart = 0;
+};
+
+// vec_out: device [dim], receives the normalised eigenvector of the lowest
+// eigenvalue.  with_resid: also the direct residuals |H x_i - theta_i x_i|
+// of the nev Ritz vectors (arpack_solver.f90:94-101), three more H.v.
+void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec_out, ArpackOut& R,
+                      bool with_resid)
+{
+    const long long n = S.dim;
+    if (n < kArNcv) throw EdztError{EDZT_ERR_ARG, "diag_arpack: sector dimension below ncv = 6"};
+    const int m = kArNcv, kmax = kArNev + (kArNcv - kArNev) / 2;
+    const double eps = 0x1p-53, eps23 = std::pow(eps, 2.0 / 3.0), tol = eps;
+    cudaStream_t st = c->stream;
+    Lease<double> buf(c->pool, (size_t)(m + 1 + kmax) * n);
+    Lease<double> small(c->pool, (size_t)rl_partials_size() + 32 + EDZT_RL_MAXV * EDZT_RL_MAXV);
+    double* part = small.p;
+    double* hd = small.p + rl_partials_size();          // [0, 8) pass 1, [8, 16) pass 2, [16] |w|^2
+    double* Yd = hd + 32;
+    std::vector<double*> spare;
+    for (int i = m + 1 + kmax - 1; i >= 0; i--) spare.push_back(buf.p + (size_t)i * n);
+    auto take = [&] { double* p = spare.back(); spare.pop_back(); return p; };
+    std::vector<double*> V(m + 1, nullptr);
+    double T[kArNcv][kArNcv] = {};
+    double* hh = c->pinned;                              // 17 host doubles
+    // orthogonalise w against V[0..nv) twice; returns |w|^2, projections in hh
+    auto orth = [&](double* w, int nv) {
+        RlVecs B{};
+        for (int q = 0; q < nv; q++) B.p[q] = V[q];
+        if (nv > 0) {
+            launch_rl_mdot(B, nv, w, n, part, hd, st);
+            launch_rl_project_out(w, B, nv, hd, n, st);
+            launch_rl_mdot(B, nv, w, n, part, hd + 8, st);
+            launch_rl_project_out(w, B, nv, hd + 8, n, st);
+            g_launches += 6;
+        }
+        RlVecs W{};
+        W.p[0] = w;
+        launch_rl_mdot(W, 1, w, n, part, hd + 16, st);
+        g_launches += 2;
+        CKLAUNCH();
+        CK(cudaMemcpyAsync(hh, hd, sizeof(double) * 17, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return hh[16];
+    };
+    // a random unit vector orthogonal to V[0..nv) into V[nv]
+    auto random_vector = [&](int nv, uint64_t stream_no) {
+        for (int tries = 0; tries < 3; tries++) {
+            launch_fill_start(V[nv], n, edzt_stream_key(key, stream_no + (uint64_t)tries), st);
+            g_launches += 1;
+            const double nrm2 = orth(V[nv], nv);
+            if (nrm2 > 0.0) {
+                launch_rl_div(V[nv], V[nv], std::sqrt(nrm2), n, st);
+                g_launches += 1;
+                return;
+            }
+        }
+        throw EdztError{EDZT_ERR_NUMERIC, "diag_arpack: no start vector orthogonal to the basis"};
+    };
+    V[0] = take();
+    random_vector(0, 0);
+    int k = 0;                                           // basis vectors carried over by the last restart
+    double anorm = 0.0, betam = 0.0;
+    std::vector<double> theta(m), Y((size_t)m * m);
+    for (;;) {
+        for (int j = k; j < m; j++) {                    // extend the factorisation to m vectors
+            if (!V[j + 1]) V[j + 1] = take();
+            double* w = V[j + 1];
+            launch_hx(S, V[j], w, 0, st);
+            g_launches += 1;
+            R.nmult++;
+            const double nrm2 = orth(w, j + 1);
+            T[j][j] = hh[j] + hh[8 + j];
+            const double beta = std::sqrt(std::max(nrm2, 0.0));
+            anorm = std::max(anorm, std::fabs(T[j][j]) + beta + (j > 0 ? std::fabs(T[j - 1][j]) : 0.0));
+            const bool invariant = !(beta > 1e-13 * anorm);
+            if (j + 1 < m) {
+                if (invariant) {                          // invariant subspace: restart the recursion
+                    random_vector(j + 1, 1000 + (uint64_t)R.nmult);
+                    T[j][j + 1] = T[j + 1][j] = 0.0;
+                } else {
+                    launch_rl_div(w, w, beta, n, st);
+                    g_launches += 1;
+                    T[j][j + 1] = T[j + 1][j] = beta;
+                }
+            } else {
+                betam = invariant ? 0.0 : beta;
+                if (!invariant) {
+                    launch_rl_div(w, w, beta, n, st);
+                    g_launches += 1;
+                }
+            }
+        }
+        double A[kArNcv * kArNcv];
+        for (int i = 0; i < m; i++)
+            for (int j = 0; j < m; j++) A[i * m + j] = T[i][j];
+        if (edzt::symmetric_eig(m, A, theta.data(), Y.data()) != 0)
+            throw EdztError{EDZT_ERR_NUMERIC, "diag_arpack: non-finite projected matrix"};
+        int nconv = 0;
+        for (int i = 0; i < kArNev; i++) {
+            R.ritz[i] = theta[i];
+            R.bounds[i] = std::fabs(betam * Y[(size_t)(m - 1) * m + i]);
+            if (R.bounds[i] <= tol * std::max(eps23, std::fabs(theta[i]))) nconv++;
+        }
+        if (nconv >= kArNev) break;
+        if (++R.nrestart > kArMaxItr)
+            throw EdztError{EDZT_ERR_NUMERIC, "diag_arpack: not converged in 20000 restarts"};
+        // thick restart: V[0..kk) = Ritz vectors, V[kk] = residual, T = arrow
+        const int kk = kArNev + std::min(nconv, (kArNcv - kArNev) / 2);
+        std::vector<double> Yk((size_t)m * kk);
+        for (int j = 0; j < m; j++)
+            for (int i = 0; i < kk; i++) Yk[(size_t)j * kk + i] = Y[(size_t)j * m + i];
+        CK(cudaMemcpyAsync(Yd, Yk.data(), sizeof(double) * Yk.size(), cudaMemcpyHostToDevice, st));
+        RlVecs B{};
+        RlOut O{};
+        for (int j = 0; j < m; j++) B.p[j] = V[j];
+        for (int i = 0; i < kk; i++) O.p[i] = take();
+        launch_rl_combine(O, kk, B, m, Yd, n, st);
+        g_launches += 1;
+        CKLAUNCH();
+        CK(cudaStreamSynchronize(st));                   // Yk (pageable) consumed
+        double* resid_vec = V[m];
+        for (int j = 0; j < m; j++) spare.push_back(V[j]);
+        std::fill(V.begin(), V.end(), nullptr);
+        for (int i = 0; i < kk; i++) V[i] = O.p[i];
+        V[kk] = resid_vec;
+        for (int i = 0; i < m; i++)
+            for (int j = 0; j < m; j++) T[i][j] = 0.0;
+        for (int i = 0; i < kk; i++) {
+            T[i][i] = theta[i];
+            T[i][kk] = T[kk][i] = betam * Y[(size_t)(m - 1) * m + i];
+        }
+        if (betam == 0.0) random_vector(kk, 2000000 + (uint64_t)R.nrestart);
+        k = kk;
+    }
+    // Ritz vectors (dseupd): the lowest into vec_out, normalised
+    const int nvec = with_resid ? kArNev : 1;
+    std::vector<double> Yk((size_t)m * nvec);
+    for (int j = 0; j < m; j++)
+        for (int i = 0; i < nvec; i++) Yk[(size_t)j * nvec + i] = Y[(size_t)j * m + i];
+    CK(cudaMemcpyAsync(Yd, Yk.data(), sizeof(double) * Yk.size(), cudaMemcpyHostToDevice, st));
+    RlVecs B{};
+    RlOut O{};
+    for (int j = 0; j < m; j++) B.p[j] = V[j];
+    O.p[0] = vec_out;
+    for (int i = 1; i < nvec; i++) O.p[i] = take();
+    launch_rl_combine(O, nvec, B, m, Yd, n, st);
+    g_launches += 1;
+    CKLAUNCH();
+    for (int i = 0; i < nvec; i++) {
+        const double nrm2 = orth(O.p[i], 0);             // |x_i|^2 only
+        launch_rl_div(O.p[i], O.p[i], std::sqrt(nrm2), n, st);
+        g_launches += 1;
+        if (with_resid) {
+            double* w = spare.back();
+            launch_hx(S, O.p[i], w, 0, st);
+            launch_axpy(w, O.p[i], n, nullptr, theta[i], -1.0, st);
+            g_launches += 2;
+            R.resid[i] = std::sqrt(std::max(orth(w, 0), 0.0));
+        }
+    }
+    R.eigval = theta[0];
+}
+
 struct SectorResult {
     int nstep = 0;
     double e = HUGE_VAL;
     std::vector<double> a, b, coeff;
     bool ok = false;
 };
+
+// ground_state with diag_solver = 2: diag_arpack on every sector, the lowest
+// kept with the same strict rule and tie band as the Lanczos path.
+void ground_state_arpack(edzt_ctx* c, int nsector, const int* sectors, uint64_t seed, int* isector, double* e0,
+                         double* gsvec, double* e_sector, const uint64_t* streams)
+{
+    int best = -1;
+    double beste = HUGE_VAL;
+    for (int i = 0; i < nsector; i++) {
+        const int nu = sectors[2 * i], nd = sectors[2 * i + 1];
+        if (e_sector) e_sector[i] = NAN;
+        const long long dim = sector_dim(c, nu, nd);
+        if (dim <= 0) continue;
+        DevSector S = make_sector(c, nu, nd);
+        Lease<double> vec(c->pool, (size_t)dim);
+        ArpackOut R;
+        diag_arpack_impl(c, S, edzt_stream_key(seed, streams ? streams[i] : (uint64_t)i), vec.p, R, false);
+        if (e_sector) e_sector[i] = R.eigval;
+        const double tie = 1.0e-10 * std::max(1.0, std::fabs(beste));
+        if (best < 0 || R.eigval < beste - tie) {
+            best = i;
+            beste = R.eigval;
+            c->gs_residual = finish_eigvec(c, S, vec.p, R.eigval);
+            c->gs_vec = std::move(vec);
+            c->gs_up = nu; c->gs_dn = nd; c->gs_isector = i; c->gs_e0 = R.eigval;
+        }
+    }
+    if (best < 0) throw EdztError{EDZT_ERR_NUMERIC, "no sector produced a ground state"};
+    c->has_gs = true;
+    *isector = c->gs_isector;
+    *e0 = c->gs_e0;
+    if (gsvec) copy_out(c, gsvec, c->gs_vec.p, sizeof(double) * sector_dim(c, c->gs_up, c->gs_dn));
+    CK(cudaStreamSynchronize(c->stream));
+}
 
 // streams (nullable): start-vector stream of each sector; default stream i for sector i.
 void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnstep, uint64_t seed, int* isector,
@@ -725,10 +946,12 @@ void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnste
     arg_check(nsector >= 1 && sectors != nullptr, "nsector >= 1 and sectors required");
     arg_check(maxnstep >= 1, "maxnstep >= 1");
     for (int i = 0; i < nsector; i++) check_sector(c, sectors[2 * i], sectors[2 * i + 1]);
-    std::vector<SectorResult> res(nsector);
-    const int ns = nsite_of(c);
-    (void)ns;
     c->has_gs = false;
+    if (c->diag_solver == EDZT_DIAG_ARPACK) {
+        ground_state_arpack(c, nsector, sectors, seed, isector, e0, gsvec, e_sector, streams);
+        return;
+    }
+    std::vector<SectorResult> res(nsector);
     if (c->engine == EDZT_ENGINE_FUSED) {
         std::vector<JobSpec> specs;
         std::vector<int> which;
@@ -1931,15 +2154,54 @@ int edzt_diag_lanczos(edzt_ctx* c, int ne_up, int ne_dn, int maxnstep, uint64_t 
         arg_check(eigval != nullptr && maxnstep >= 1, "bad arguments");
         const long long dim = sector_dim(c, ne_up, ne_dn);
         arg_check(dim > 0, "empty sector");
-        // a one-sector ground_state on the requested start-vector stream
+        // a one-sector ground_state on the requested start-vector stream, always by Lanczos
         std::vector<int> sec = {ne_up, ne_dn};
         int is = 0;
         double e0 = 0.0;
+        struct Keep {
+            edzt_ctx* c;
+            int solver;
+            ~Keep() { c->diag_solver = solver; }
+        } keep{c, c->diag_solver};
+        c->diag_solver = EDZT_DIAG_LANCZOS;
         ground_state_impl(c, 1, sec.data(), maxnstep, seed, &is, &e0, nullptr, nullptr, &stream);
         *eigval = e0;
         if (eigvec) copy_out(c, eigvec, c->gs_vec.p, sizeof(double) * dim);
         if (residual) *residual = c->gs_residual;
         CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int edzt_diag_arpack(edzt_ctx* c, int ne_up, int ne_dn, uint64_t seed, uint64_t stream, double* eigval,
+                     double* eigvec, double* ritz, double* resid, int* nmult)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        check_sector(c, ne_up, ne_dn);
+        arg_check(eigval != nullptr, "eigval required");
+        const long long dim = sector_dim(c, ne_up, ne_dn);
+        arg_check(dim > 0, "empty sector");
+        DevSector S = make_sector(c, ne_up, ne_dn);
+        Lease<double> vec(c->pool, (size_t)dim);
+        ArpackOut R;
+        diag_arpack_impl(c, S, edzt_stream_key(seed, stream), vec.p, R, resid != nullptr);
+        *eigval = R.eigval;
+        for (int i = 0; i < kArNev; i++) {
+            if (ritz) ritz[i] = R.ritz[i];
+            if (resid) resid[i] = R.resid[i];
+        }
+        if (nmult) *nmult = R.nmult;
+        if (eigvec) copy_out(c, eigvec, vec.p, sizeof(double) * dim);
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int edzt_set_diag_solver(edzt_ctx* c, int diag_solver)
+{
+    return guarded(c, [&] {
+        if (diag_solver != EDZT_DIAG_LANCZOS && diag_solver != EDZT_DIAG_ARPACK)
+            throw EdztError{EDZT_ERR_ARG, "invalid diag solver"};
+        c->diag_solver = diag_solver;
     });
 }
 

@@ -66,6 +66,20 @@ struct CFJob {
 void launch_cf(const CFJob* jobs_dev, int njobs, const double* omega, int nw, cudaStream_t s, int real_axis = 0,
                double eta = 0.0);
 
+// ---- arpack.cu: vector kernels of the restarted Lanczos (diag_arpack) ------
+#define EDZT_RL_MAXV 8
+struct RlVecs { const double* p[EDZT_RL_MAXV]; };
+struct RlOut { double* p[EDZT_RL_MAXV]; };
+int rl_partials_size();
+// out[q] = <V_q, w> for q < nv (device, deterministic); partials: rl_partials_size() doubles.
+void launch_rl_mdot(const RlVecs& V, int nv, const double* w, long long n, double* partials, double* out,
+                    cudaStream_t s);
+// w -= sum_q h[q] V_q (h on the device).
+void launch_rl_project_out(double* w, const RlVecs& V, int nv, const double* h, long long n, cudaStream_t s);
+// O_i = sum_{j<m} Y[j*k + i] V_j for i < k (Y on the device, m, k <= EDZT_RL_MAXV).
+void launch_rl_combine(const RlOut& O, int k, const RlVecs& V, int m, const double* Y, long long n, cudaStream_t s);
+void launch_rl_div(double* out, const double* w, double beta, long long n, cudaStream_t s);
+
 // ---- lanczos.cu: persistent fused Lanczos over a batch of jobs ------------
 enum LzMode { LZ_COEFF = 0, LZ_EIGVEC = 1 };
 enum LzInit { LZ_INIT_HASH = 0, LZ_INIT_APPLYC = 1, LZ_INIT_COPY = 2 };

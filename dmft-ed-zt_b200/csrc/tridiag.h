@@ -106,4 +106,62 @@ inline int lowest_eigenpair(int n, const double* d, const double* e, double* lam
     return 0;
 }
 
+// All eigenpairs of a small dense symmetric matrix by the cyclic Jacobi
+// method (Golub & Van Loan, Matrix Computations, §8.5): rotations
+// annihilate each off-diagonal element in turn until the off-diagonal part
+// is negligible against the diagonal.  A: row-major m x m (overwritten).
+// w: eigenvalues ascending; Z: row-major, column i the eigenvector of w[i].
+// For the projected matrix of the restarted Lanczos, m <= 8.
+inline int symmetric_eig(int m, double* A, double* w, double* Z)
+{
+    if (m < 1) return -1;
+    for (int i = 0; i < m * m; i++)
+        if (!std::isfinite(A[i])) return -2;
+    std::vector<double> V((size_t)m * m, 0.0);
+    for (int i = 0; i < m; i++) V[(size_t)i * m + i] = 1.0;
+    auto a = [&](int i, int j) -> double& { return A[(size_t)i * m + j]; };
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < m; i++) {
+            diag += a(i, i) * a(i, i);
+            for (int j = i + 1; j < m; j++) off += a(i, j) * a(i, j);
+        }
+        if (off <= 1e-34 * diag || off == 0.0) break;
+        for (int p = 0; p < m; p++)
+            for (int q = p + 1; q < m; q++) {
+                const double apq = a(p, q);
+                if (apq == 0.0) continue;
+                const double th = (a(q, q) - a(p, p)) / (2.0 * apq);
+                const double t = (th >= 0.0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < m; k++) {            // A = J^T A J
+                    const double akp = a(k, p), akq = a(k, q);
+                    a(k, p) = c * akp - s * akq;
+                    a(k, q) = s * akp + c * akq;
+                }
+                for (int k = 0; k < m; k++) {
+                    const double apk = a(p, k), aqk = a(q, k);
+                    a(p, k) = c * apk - s * aqk;
+                    a(q, k) = s * apk + c * aqk;
+                }
+                a(p, q) = a(q, p) = 0.0;
+                for (int k = 0; k < m; k++) {
+                    const double vkp = V[(size_t)k * m + p], vkq = V[(size_t)k * m + q];
+                    V[(size_t)k * m + p] = c * vkp - s * vkq;
+                    V[(size_t)k * m + q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    std::vector<int> order(m);
+    for (int i = 0; i < m; i++) order[i] = i;
+    for (int i = 1; i < m; i++)                          // insertion sort by eigenvalue
+        for (int j = i; j > 0 && a(order[j], order[j]) < a(order[j - 1], order[j - 1]); j--)
+            std::swap(order[j], order[j - 1]);
+    for (int i = 0; i < m; i++) {
+        w[i] = a(order[i], order[i]);
+        for (int k = 0; k < m; k++) Z[(size_t)k * m + i] = V[(size_t)k * m + order[i]];
+    }
+    return 0;
+}
+
 }  // namespace edzt

@@ -127,6 +127,29 @@ int edzt_lanczos_iteration_noalloc(edzt_ctx *ctx, int ne_up, int ne_dn, const do
 int edzt_diag_lanczos(edzt_ctx *ctx, int ne_up, int ne_dn, int maxnstep, uint64_t seed, uint64_t stream,
                       double *eigval, double *eigvec, double *residual);
 
+/* diag_arpack (src/arpack_solver.f90:19-124): lowest eigenvalue and
+ * eigenvector of a sector by a restarted Lanczos with the reference's ARPACK
+ * settings (nev 3, ncv 6, which 'SA', tol 0 = machine precision, exact
+ * shifts, at most 20000 restarts), kept by thick restart, which spans the
+ * same subspace as ARPACK's implicit restart with exact shifts.  The start
+ * vector is U[0,1) from (seed, stream) where ARPACK draws its own.  eigvec
+ * (nullable, host or device) [dim] is normalised; its sign is arbitrary, as
+ * ARPACK's.  ritz (nullable) [3]: the three lowest Ritz values; resid
+ * (nullable) [3]: their direct residuals |H x - theta x| (the reference's
+ * printed d(:,2)), three more H.v; nmult (nullable): H.v count (multcount).
+ * Sector dimension < ncv = 6: EDZT_ERR_ARG (pdsaupd rejects it); not
+ * converged in 20000 restarts: EDZT_ERR_NUMERIC (the reference dies). */
+int edzt_diag_arpack(edzt_ctx *ctx, int ne_up, int ne_dn, uint64_t seed, uint64_t stream, double *eigval,
+                     double *eigvec, double *ritz, double *resid, int *nmult);
+
+/* ground_state's diag_solver (src/ground_state.f90:53-60): 1 = diag_lanczos
+ * (default), 2 = diag_arpack on every sector; anything else EDZT_ERR_ARG
+ * ("invalid diag solver").  Applies to edzt_ground_state and edzt_solve;
+ * edzt_diag_lanczos, the batched and the served forms always use Lanczos. */
+#define EDZT_DIAG_LANCZOS 1
+#define EDZT_DIAG_ARPACK 2
+int edzt_set_diag_solver(edzt_ctx *ctx, int diag_solver);
+
 /* ground_state (src/ground_state.f90:1-81): scans sectors[nsector][2] =
  * (ne_up, ne_dn), keeps the lowest energy (a later sector wins only if lower
  * by more than 1e-10*max(1,|E|)), and keeps its normalised vector resident

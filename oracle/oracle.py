@@ -346,6 +346,38 @@ class Oracle:
             return 0.5 * (gm[0:1] + gm[1:2])
         return gm
 
+    def diag_arpack(self, ne_up, ne_dn, seed=0, stream=0):
+        """diag_arpack (src/arpack_solver.f90:19-124) through ARPACK itself:
+        scipy's eigsh wraps ARPACK's dsaupd/dseupd, the serial form of the
+        reference's pdsaupd/pdseupd, here with the reference's settings
+        (nev 3, ncv 6, which 'SA', tol 0, maxitr 20000) on this oracle's hx
+        and the library's start vector (ARPACK would draw its own)."""
+        from scipy.sparse.linalg import LinearOperator, eigsh
+        n = self.dim(ne_up, ne_dn)
+        op = LinearOperator((n, n), matvec=lambda x: self.hx(ne_up, ne_dn, np.ascontiguousarray(x, dtype=float)),
+                            dtype=float)
+        w, v = eigsh(op, k=3, ncv=6, which="SA", tol=0.0, maxiter=20000,
+                     v0=start_vector(seed, stream, n))
+        order = np.argsort(w)
+        w, v = w[order], v[:, order]
+        resid = np.array([np.linalg.norm(self.hx(ne_up, ne_dn, v[:, i].copy()) - w[i] * v[:, i]) for i in range(3)])
+        return dict(e0=float(w[0]), vec=v[:, 0].copy(), ritz=w, resid=resid)
+
+    def ground_state_arpack(self, sectors, seed=0):
+        """ground_state with diag_solver = 2 (ground_state.f90:53-68): the
+        lowest diag_arpack energy over the sectors, sector i on stream i."""
+        best = None
+        es = np.full(len(sectors), np.nan)
+        for i, (u, d) in enumerate(sectors):
+            if self.dim(u, d) <= 0:
+                continue
+            r = self.diag_arpack(u, d, seed, i)
+            es[i] = r["e0"]
+            if best is None or r["e0"] < best[1] - 1e-10 * max(1.0, abs(best[1])):
+                best = (i, r["e0"], r["vec"])
+        i, e0, vec = best
+        return dict(isector=i, e0=e0, vec=vec, e_sector=es, sector=tuple(int(x) for x in sectors[i]))
+
     def dense_h(self, ne_up, ne_dn) -> np.ndarray:
         """H assembled column by column from hx (the idea of debug.f90:13-57)."""
         n = self.dim(ne_up, ne_dn)

@@ -211,3 +211,19 @@ def test_edge_cases(pkg, oracle_mod):
     v1 = oracle_mod.start_vector(5, 0, 1000)
     assert np.all((v1 >= 0) & (v1 < 1)) and np.array_equal(v1, oracle_mod.start_vector(5, 0, 1000))
     assert not np.array_equal(v1, oracle_mod.start_vector(5, 1, 1000))
+
+
+def test_arpack_oracle_matches_dense(pkg, oracle_mod):
+    """The oracle's ARPACK path (scipy's eigsh = ARPACK dsaupd/dseupd) against
+    dense diagonalisation: lowest three eigenvalues and the ground state."""
+    m = random_model(pkg, np.random.default_rng(31), 2, 3, J=0.4)
+    o = oracle_for(oracle_mod, m)
+    r = o.diag_arpack(2, 3, seed=1, stream=0)
+    w, v = np.linalg.eigh(o.dense_h(2, 3))
+    assert np.abs(r["ritz"] - w[:3]).max() <= 1e-12 * max(1.0, abs(w[0]))
+    assert abs(abs(r["vec"] @ v[:, 0]) - 1.0) <= 1e-12
+    assert r["resid"].max() <= 1e-12
+    gs = o.ground_state_arpack([(2, 3), (3, 3), (3, 2)], seed=1)
+    es = [np.linalg.eigvalsh(o.dense_h(u, d))[0] for u, d in [(2, 3), (3, 3), (3, 2)]]
+    assert np.abs(gs["e_sector"] - es).max() <= 1e-12 * max(1.0, abs(min(es)))
+    assert abs(gs["e0"] - min(es)) <= 1e-12 * max(1.0, abs(min(es)))
