@@ -509,6 +509,65 @@ def run_gpu(args):
     return 0
 
 
+def run_case(spec, steps):
+    """Small single-kernel workloads for ncu captures and kernel A/B timing,
+    on the half-filled sector of the hv leg's single-orbital model at nsite NS:
+      hx:NS   four y = H x calls (k_hx); the last one is timed
+      lz:NS   lanczos_iteration of 5, then of `steps` steps (k_lanczos); the
+              second launch is timed
+      solve   one impurity solve of the bench workload (nsite 12, 9 sectors)
+    Prints one JSON line with the device time (CUDA events) of the timed part."""
+    import numpy as np
+    import torch
+
+    pkg = load_pkg()
+    s = pkg.Solver(0)
+    kind, _, arg = spec.partition(":")
+    out = {"case": spec}
+    if kind == "solve":
+        cfg = workload()
+        s.set_model(cfg["model"])
+        omega = pkg.matsubara(cfg["nw"], cfg["beta"])
+        s.solve(cfg["sectors"], cfg["maxnstep"], omega, nspin=1, seed=0)
+        s.reset_stats()
+        s.solve(cfg["sectors"], cfg["maxnstep"], omega, nspin=1, seed=0)
+        st = s.kernel_stats()
+        out.update(k_lanczos_ms=st["ms"], launches=st["launches"])
+    else:
+        ns = int(arg)
+        nb = ns - 1
+        rng = np.random.default_rng(ns)
+        m = pkg.Model(1, nb, np.zeros((1, 2)), np.stack([rng.uniform(-2, 2, nb)] * 2, 1),
+                      np.stack([rng.uniform(0.1, 1, nb)] * 2, 1).reshape(1, nb, 2), U=3.0, mu=1.5)
+        s.set_model(m)
+        n = s.dim(ns // 2, ns // 2)
+        out["dim"] = int(n)
+        if kind == "hx":
+            stream = torch.cuda.ExternalStream(s.stream_ptr())
+            x = torch.rand(n, dtype=torch.float64, device="cuda")
+            y = torch.empty_like(x)
+            for _ in range(3):
+                s.hx(ns // 2, ns // 2, x, y)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.hx(ns // 2, ns // 2, x, y)
+            e1.record(stream)
+            e1.synchronize()
+            out["k_hx_ms"] = e0.elapsed_time(e1)
+        elif kind == "lz":
+            v0 = np.random.default_rng(0).random(n)
+            s.lanczos_iteration(ns // 2, ns // 2, v0, 5)
+            s.reset_stats()
+            s.lanczos_iteration(ns // 2, ns // 2, v0, steps)
+            st = s.kernel_stats()
+            out.update(steps=steps, k_lanczos_ms=st["ms"], ns_per_state_step=st["ms"] * 1e6 / (n * (steps + 1)))
+        else:
+            raise SystemExit(f"unknown case {spec}")
+    s.close()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -521,7 +580,10 @@ def main():
     ap.add_argument("--batched", type=int, default=64, help="instances of the batched leg (0: skip)")
     ap.add_argument("--served", type=int, default=32, help="requests of the served leg (0: skip)")
     ap.add_argument("--traffic-file", default=os.path.join(ROOT, "profiles", "k_lanczos_aim_n12_dram.txt"))
+    ap.add_argument("--case", default=None, help="run one small profiling case (hx:NS, lz:NS, solve) and exit")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args.case, args.steps)
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)
