@@ -5,7 +5,6 @@
 #include "edzt_internal.h"
 #include "hv_row.cuh"
 
-static constexpr int kHxThreads = 256;
 static constexpr size_t kHxSmemTarget = 24 * 1024;
 static constexpr int kWintDoubles = EDZT_MAX_P * EDZT_MAX_P;
 static constexpr int kAmpDoubles = EDZT_MAX_AMP;
@@ -30,10 +29,12 @@ int hx_rows_per_tile(int nup, int ndn, int hw_dn)
 // H.v: y = H x (accumulate = 0) or y = y + H x (accumulate = 1), the `py`
 // flag of src/impurity_hamiltonian.f90:241-245.  One CTA per block of R full
 // rows; the rows and their per-row hop data are staged in shared memory.
+// T threads per CTA: 256, or for large sectors 512 (two CTAs per SM) and
+// 1024 (one), both at 64 registers, 32 warps per SM.
 // ---------------------------------------------------------------------------
-template <bool ACC>
-__global__ void __launch_bounds__(kHxThreads) k_hx(DevSector S, const double* __restrict__ x,
-                                                   double* __restrict__ y, int R)
+template <bool ACC, int T>
+__global__ void __launch_bounds__(T, T == 512 ? 2 : 1) k_hx(DevSector S, const double* __restrict__ x,
+                                                           double* __restrict__ y, int R)
 {
     extern __shared__ __align__(16) double smem[];
     double* wint = smem;
@@ -67,6 +68,32 @@ __global__ void __launch_bounds__(kHxThreads) k_hx(DevSector S, const double* __
     }
 }
 
+// Threads per CTA of k_hx by sector dimension.  Measured on B200 (y = H x on
+// the half-filled sector of a single-orbital impurity): at nsite 16 (1.66e8
+// states) 4.45 / 3.10 / 2.85 ms with 256 / 512 / 1024 threads, at nsite 14
+// (1.18e7) 0.228 / 0.212 / 0.254 ms, at nsite 12 (8.5e5) 0.039 / 0.040 /
+// 0.042 ms.  Large sectors wait on the latency of their down-hop gathers,
+// which more warps per SM hide; small ones have too few row tiles to fill
+// 148 SMs with large CTAs.
+int hx_threads(long long dim)
+{
+    return dim >= (32LL << 20) ? 1024 : dim >= (4LL << 20) ? 512 : 256;
+}
+
+template <int T>
+static void launch_hx_t(const DevSector& S, const double* x, double* y, int accumulate, int tiles, int R,
+                        size_t smem, cudaStream_t s)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_hx<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_hx<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_set = true;
+    }
+    if (accumulate) k_hx<true, T><<<tiles, T, smem, s>>>(S, x, y, R);
+    else k_hx<false, T><<<tiles, T, smem, s>>>(S, x, y, R);
+}
+
 void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s)
 {
     const int nup = S.up.count, ndn = S.dn.count;
@@ -74,14 +101,11 @@ void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, c
     const int R = hx_rows_per_tile(nup, ndn, S.dn.hw);
     const int tiles = (ndn + R - 1) / R;
     const size_t smem = (kWintDoubles + kAmpDoubles) * sizeof(double) + (size_t)R * staged_row_bytes(nup, S.dn.hw);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_hx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        cudaFuncSetAttribute(k_hx<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr_set = true;
+    switch (hx_threads(S.dim)) {
+    case 1024: launch_hx_t<1024>(S, x, y, accumulate, tiles, R, smem, s); break;
+    case 512: launch_hx_t<512>(S, x, y, accumulate, tiles, R, smem, s); break;
+    default: launch_hx_t<256>(S, x, y, accumulate, tiles, R, smem, s); break;
     }
-    if (accumulate) k_hx<true><<<tiles, kHxThreads, smem, s>>>(S, x, y, R);
-    else k_hx<false><<<tiles, kHxThreads, smem, s>>>(S, x, y, R);
 }
 
 // ---------------------------------------------------------------------------
