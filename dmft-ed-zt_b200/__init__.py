@@ -52,7 +52,7 @@ EXPORTS = (
     "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
     "edzt_cluster_green_matrix", "edzt_gs_occupancy", "edzt_green_real", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
     "edzt_server_cancel", "edzt_instance_footprint", "edzt_set_fault_test", "edzt_diag_arpack",
-    "edzt_set_diag_solver",
+    "edzt_set_diag_solver", "edzt_hybridization", "edzt_local_green_bethe", "edzt_fit_bath", "edzt_dmft_bethe",
 )
 # ground_state's diag_solver values (src/ground_state.f90:53-60).
 DIAG_LANCZOS = 1
@@ -78,6 +78,16 @@ def _instance(inst, keep):
     keep += [em, ek, vmk, sec]
     return Instance(m.norb, m.nbath, em.ctypes.data, ek.ctypes.data, vmk.ctypes.data, m.U, m.Up, m.Jex, m.Jp, m.mu,
                     len(sec), sec.ctypes.data, int(inst.get("nspin", 1)), int(inst.get("seed", 0)))
+
+
+class DMFTParams(C.Structure):
+    """edzt_dmft_params of include/edzt.h: settings of the DMFT loop."""
+    _fields_ = [("norb", C.c_int), ("nbath", C.c_int), ("nspin", C.c_int),
+                ("U", C.c_double), ("Up", C.c_double), ("Jex", C.c_double), ("Jp", C.c_double),
+                ("mu", C.c_double), ("hfield", C.c_double), ("nsector", C.c_int), ("sectors", C.c_void_p),
+                ("maxnstep", C.c_int), ("seed", C.c_uint64), ("nw", C.c_int), ("omega", C.c_void_p),
+                ("nloop", C.c_int), ("scf_tol", C.c_double), ("mixing", C.c_double), ("fit_ftol", C.c_double),
+                ("outdir", C.c_char_p)]
 
 
 class EDError(RuntimeError):
@@ -141,6 +151,10 @@ def load_library(path: str = LIB_PATH):
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
     L.edzt_diag_arpack.argtypes = [_vp, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _vp, _vp, _ip]
     L.edzt_set_diag_solver.argtypes = [_vp, C.c_int]
+    L.edzt_hybridization.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp]
+    L.edzt_local_green_bethe.argtypes = [C.c_int, C.c_int, C.c_int, _vp, C.c_double, _vp, _vp, _vp]
+    L.edzt_fit_bath.argtypes = [C.c_int] * 4 + [_vp] * 7 + [C.c_double, _vp]
+    L.edzt_dmft_bethe.argtypes = [_vp, C.POINTER(DMFTParams)] + [_vp] * 7 + [_ip, _vp, _ip]
     L.edzt_ground_state.argtypes = [_vp, C.c_int, _vp, C.c_int, C.c_uint64, _ip, _dp, _vp, _vp]
     L.edzt_gs_dim.argtypes = [_vp]
     L.edzt_gs_dim.restype = C.c_longlong
@@ -195,6 +209,56 @@ class Model:
         return (np.ascontiguousarray(self.em.ravel(order="F")),
                 np.ascontiguousarray(self.ek.ravel(order="F")),
                 np.ascontiguousarray(self.vmk.ravel(order="F")))
+
+
+def _host_check(rc: int, what: str):
+    if rc != EDZT_OK:
+        raise EDError(rc, what)
+
+
+def _cplx_f(G) -> np.ndarray:
+    """Complex [nspin][norb][nw] as the interleaved Fortran array (nw, norb, nspin)."""
+    return np.ascontiguousarray(np.asarray(G, dtype=np.complex128)).view(np.float64).ravel()
+
+
+def hybridization(ek, vmk, omega, nspin) -> np.ndarray:
+    """D_cl[ispin, iorb, iw] by the library (edzt_hybridization); no device needed."""
+    ek, vmk, omega = (np.asarray(a, dtype=np.float64) for a in (ek, vmk, omega))
+    norb, nbath = vmk.shape[0], vmk.shape[1]
+    D = np.zeros((nspin, norb, omega.size), dtype=np.complex128)
+    ekf, vmf, om = (np.ascontiguousarray(a.ravel(order="F")) for a in (ek, vmk, omega))
+    _host_check(load_library().edzt_hybridization(norb, nbath, nspin, omega.size, _ptr(om), _ptr(ekf), _ptr(vmf),
+                                                  D.ctypes.data), "edzt_hybridization")
+    return D
+
+
+def local_green_bethe(em, D, G_cl, hfield=0.0) -> np.ndarray:
+    """G_loc[ispin, iorb, iw] of the Bethe lattice by the library (edzt_local_green_bethe)."""
+    em = np.ascontiguousarray(np.asarray(em, dtype=np.float64).ravel(order="F"))
+    nspin, norb, nw = np.shape(G_cl)
+    G = np.zeros((nspin, norb, nw), dtype=np.complex128)
+    Df, Gf = _cplx_f(D), _cplx_f(G_cl)
+    _host_check(load_library().edzt_local_green_bethe(norb, nspin, nw, _ptr(em), float(hfield), _ptr(Df), _ptr(Gf),
+                                                      G.ctypes.data), "edzt_local_green_bethe")
+    return G
+
+
+def fit_bath(em, ek, vmk, D, G_cl, G_loc, omega, nspin, ftol=1.0e-6):
+    """New (em, ek, vmk) by the library's conjugate-gradient bath fit
+    (edzt_fit_bath); returns them with the final cost per spin."""
+    em = np.array(em, dtype=np.float64)
+    ek = np.array(ek, dtype=np.float64)
+    vmk = np.array(vmk, dtype=np.float64)
+    norb, nbath = vmk.shape[0], vmk.shape[1]
+    omega = _f64(omega)
+    emf, ekf, vmf = (np.ascontiguousarray(a.ravel(order="F")) for a in (em, ek, vmk))
+    cost = np.zeros(nspin)
+    Df, Gc, Gl = _cplx_f(D), _cplx_f(G_cl), _cplx_f(G_loc)
+    _host_check(load_library().edzt_fit_bath(norb, nbath, nspin, omega.size, _ptr(omega), _ptr(emf), _ptr(ekf),
+                                             _ptr(vmf), _ptr(Df), _ptr(Gc), _ptr(Gl), float(ftol), _ptr(cost)),
+                "edzt_fit_bath")
+    return (emf.reshape(em.shape, order="F"), ekf.reshape(ek.shape, order="F"), vmf.reshape(vmk.shape, order="F"),
+            cost)
 
 
 def matsubara(nw: int, beta: float) -> np.ndarray:
@@ -377,6 +441,32 @@ class Solver:
                                                    _ptr(coeffs)))
         Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, norb, nw)
         return dict(G_cl=Gc, coeffs=coeffs.reshape(norb, 2, 4, maxnstep))
+
+    def dmft_bethe(self, model, sectors, maxnstep, omega, nspin=1, nloop=20, scf_tol=1.0e-6, mixing=1.0,
+                   fit_ftol=1.0e-6, hfield=0.0, seed=0, outdir=None):
+        """The DMFT loop of src/dmft.f90:38-137 on the Bethe lattice, in the
+        library (edzt_dmft_bethe): starts from model's bath, returns the last
+        iteration's em[a,s], ek[l,s], vmk[a,l,s], D_cl/G_cl/G_loc[s,a,w],
+        Z[a,s], the per-iteration convergence measure and the iteration count."""
+        omega = _f64(omega)
+        sec = np.ascontiguousarray(np.asarray(sectors, dtype=np.int32).reshape(-1, 2))
+        em, ek, vmk = model.fortran_arrays()
+        em, ek, vmk = em.copy(), ek.copy(), vmk.copy()
+        norb, nbath, nw = model.norb, model.nbath, omega.size
+        P = DMFTParams(norb, nbath, nspin, model.U, model.Up, model.Jex, model.Jp, model.mu, float(hfield), len(sec),
+                       sec.ctypes.data, maxnstep, int(seed), nw, omega.ctypes.data, nloop, float(scf_tol),
+                       float(mixing), float(fit_ftol), None if outdir is None else os.fsencode(outdir))
+        D, Gc, Gl = (np.zeros((nspin, norb, nw), dtype=np.complex128) for _ in range(3))
+        Z = np.zeros(norb * nspin)
+        hist = np.zeros(nloop)
+        it, conv = C.c_int(), C.c_int()
+        self._check(self._L.edzt_dmft_bethe(self._h, C.byref(P), _ptr(em), _ptr(ek), _ptr(vmk), D.ctypes.data,
+                                            Gc.ctypes.data, Gl.ctypes.data, _ptr(Z), C.byref(it), _ptr(hist),
+                                            C.byref(conv)))
+        return dict(em=em.reshape(norb, 2, order="F"), ek=ek.reshape(nbath, 2, order="F"),
+                    vmk=vmk.reshape(norb, nbath, 2, order="F"), D_cl=D, G_cl=Gc, G_loc=Gl,
+                    Z=Z.reshape(norb, nspin, order="F"), history=hist[: it.value], iterations=it.value,
+                    converged=bool(conv.value))
 
     def green_real(self, iorb, ispin, maxnstep, omega, eta):
         """G(w + i eta) of green_diag on real frequencies; A(w) = -Im G / pi."""

@@ -272,6 +272,61 @@ int edzt_instance_footprint(const edzt_instance *inst, long long *bytes);
  * operation.  The context stays usable after either error. */
 int edzt_set_fault_test(edzt_ctx *ctx, int pass_cap, double wait_seconds, int stall_cta);
 
+/* ---- the DMFT loop around the solver (host code, dmft_loop.cpp) ----------
+ * The caller of the path, restated so that a whole DMFT run needs no
+ * Fortran: the Bethe-lattice loop of src/dmft.f90:38-137 with the bath fit
+ * of src/ed_projection.f90 and the output files of src/dump_data.f90 and
+ * src/dmft_green.f90:66-109.  Arrays in the reference's Fortran layouts:
+ * em(norb,2), ek(nbath,2), vmk(norb,nbath,2) and complex (nw,norb,nspin),
+ * column-major, real and imaginary parts interleaved. */
+
+/* D_cl = sum_l vmk^2 / (i w - ek) (cluster_hybridization_ftn,
+ * src/dmft_green.f90:24-45).  No device needed. */
+int edzt_hybridization(int norb, int nbath, int nspin, int nw, const double *omega, const double *ek,
+                       const double *vmk, double *D);
+
+/* local_green_ftn (src/dmft_green.f90:128-170): G_loc of the Bethe lattice
+ * (semicircle, half-bandwidth 1) by the reference's 10000-point quadrature.
+ * No device needed. */
+int edzt_local_green_bethe(int norb, int nspin, int nw, const double *em, double hfield, const double *D,
+                           const double *G_cl, double *G_loc);
+
+/* fit_h_imp_params (src/ed_projection.f90:23-101): new (em, ek, vmk), in
+ * place, minimising sum_{a,w} |em - em_old + D(ek,vmk) - D_old + 1/G_loc -
+ * 1/G_cl|^2 / w / (norb nw) per spin by Polak-Ribiere conjugate gradients
+ * (relative stop ftol; the reference's is 1e-6); nspin 1 copies spin up to
+ * spin down.  cost (nullable) [nspin]: the final cost.  No device needed. */
+int edzt_fit_bath(int norb, int nbath, int nspin, int nw, const double *omega, double *em, double *ek, double *vmk,
+                  const double *D, const double *G_cl, const double *G_loc, double ftol, double *cost);
+
+typedef struct edzt_dmft_params {
+    int norb, nbath, nspin;
+    double U, Up, Jex, Jp, mu, hfield;
+    int nsector;
+    const int *sectors;     /* [nsector][2]: (ne_up, ne_dn) */
+    int maxnstep;           /* LanczosSteps */
+    uint64_t seed;          /* start vectors, as edzt_ground_state */
+    int nw;
+    const double *omega;    /* [nw] Matsubara frequencies */
+    int nloop;              /* at most this many iterations */
+    double scf_tol;         /* stop when sum |G_cl - G_loc|^2 / (norb nbath nw) < scf_tol */
+    double mixing;          /* (0, 1]: new = mixing * fitted + (1 - mixing) * previous; 1 = the reference */
+    double fit_ftol;        /* bath-fit stop; 1e-6 = the reference */
+    const char *outdir;     /* nullable: write h_imp.dat, green.dat.<o>.<s>, g_coeffs.dat every
+                             * iteration and sigma.dat.<o>.<s> at the end, into this directory */
+} edzt_dmft_params;
+
+/* The DMFT loop (src/dmft.f90:55-98) with this library as the impurity
+ * solver: em, ek, vmk (in/out) start as the initial bath and return the
+ * last iteration's; D_cl, G_cl, G_loc (nullable) complex (nw,norb,nspin) of
+ * the last iteration; Z (nullable) (norb,nspin) the quasiparticle weight
+ * 1/(1 - Im Sigma(i w_1)/w_1) (src/post_process.f90:39-57, for every
+ * orbital and spin); history (nullable) [nloop] the convergence measure of
+ * each iteration; *iterations, *converged.  Errors of the solver calls are
+ * returned as they come (edzt_last_error(ctx) has the message). */
+int edzt_dmft_bethe(edzt_ctx *ctx, const edzt_dmft_params *p, double *em, double *ek, double *vmk, double *D_cl,
+                    double *G_cl, double *G_loc, double *Z, int *iterations, double *history, int *converged);
+
 /* Kernel launches issued by this context since creation (instrumentation). */
 long long edzt_launch_count(const edzt_ctx *ctx);
 

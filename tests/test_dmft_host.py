@@ -5,6 +5,7 @@ the oracle solver."""
 import importlib
 
 import numpy as np
+import pytest
 
 
 def _dmft(pkg):
@@ -89,3 +90,40 @@ def test_self_energy_vanishes_without_interaction(pkg, oracle_mod):
     S = d.self_energy(em, D, G0, w, mu)
     assert np.allclose(d.quasiparticle_weight(S, w, literal=True), 1.0)        # only (iorb 2, ispin 2) is kept
     assert d.quasiparticle_weight(S, w)[0, 0] != 1.0
+
+
+def test_library_host_loop_pieces_match_restatement(pkg, oracle_mod):
+    """The library's C++ DMFT pieces (hybridization, Bethe G_loc, bath fit;
+    no device needed) against this module's Python restatement of them."""
+    d = _dmft(pkg)
+    pkg.build()
+    rng = np.random.default_rng(8)
+    w = oracle_mod.matsubara(256, 40.0)
+    for norb, nbath, nspin in [(1, 5, 1), (2, 3, 2)]:
+        em = rng.uniform(-.5, .5, (norb, 2))
+        ek = rng.uniform(-1, 1, (nbath, 2))
+        V = rng.uniform(.2, .8, (norb, nbath, 2))
+        if nspin == 1:
+            em[:, 1], ek[:, 1], V[..., 1] = em[:, 0], ek[:, 0], V[..., 0]
+        D = d.hybridization(ek, V, w, nspin)
+        assert np.abs(pkg.hybridization(ek, V, w, nspin) - D).max() <= 1e-14
+        G_cl = 1.0 / (1j * w[None, None, :] - 0.2 - D + 0.3 / (1j * w[None, None, :] + 0.4))
+        G_loc = d.local_green(em, D, G_cl, 0.05)
+        assert np.abs(pkg.local_green_bethe(em, D, G_cl, 0.05) - G_loc).max() <= 1e-12
+        # a fit whose minimum is flat (couplings go to zero): the same cost
+        em0, ek0, V0 = em + 0.03, ek * 1.05, V * 0.95
+        emp, ekp, Vp, info = d.fit_bath(em0, ek0, V0, D, G_cl, G_loc, w, nspin, ftol=1e-13)
+        emc, ekc, Vc, cost = pkg.fit_bath(em0, ek0, V0, D, G_cl, G_loc, w, nspin, ftol=1e-13)
+        for s in range(nspin):
+            assert abs(cost[s] - info[s][1]) <= 1e-10 * info[s][1] + 1e-16
+        # with G_loc = G_cl the target is em0 + D(ek, V), which a bath of this
+        # size represents exactly: both fits return em0 and a bath giving D
+        # (the cost goes to zero, where the relative stop needs a looser ftol)
+        emc, ekc, Vc, cost = pkg.fit_bath(em0, ek0, V0, D, G_cl, G_cl, w, nspin, ftol=1e-9)
+        emp, ekp, Vp, info = d.fit_bath(em0, ek0, V0, D, G_cl, G_cl, w, nspin, ftol=1e-9)
+        assert cost.max() < 1e-12
+        for got in ((emc, ekc, Vc), (emp, ekp, Vp)):
+            assert np.abs(got[0] - em0).max() <= 1e-6
+            assert np.abs(d.hybridization(got[1], got[2], w, nspin) - D).max() <= 1e-5
+    with pytest.raises(pkg.EDError):
+        pkg.fit_bath(em, ek, V, D, G_cl, G_loc, w, nspin, ftol=0.0)

@@ -1,10 +1,13 @@
 """The CPU-runnable workload end to end: nsite-6 Bethe-lattice DMFT, 20
 iterations with linear mixing 0.5, 200 Lanczos steps, 2048 Matsubara points
-at beta 100, run by the same host loop on the GPU library and on the oracle.
-The converged hybridization D_cl(i w) must agree to 1e-6; G_cl, G_loc and the
-quasiparticle weight are held to the same bound.
+at beta 100.  The oracle run is the Python loop (dmft.py) on the CPU oracle
+solver; against it run the same Python loop on the GPU library and the
+library's own C++ loop (edzt_dmft_bethe).  The converged hybridization
+D_cl(i w) must agree to 1e-6; G_cl, G_loc and the quasiparticle weight are
+held to the same bound.  A shorter run with mixing 1 (the reference's loop,
+which has no mixing) is held to the same bound.
 
-Both loops fit the bath to a relative tolerance of 1e-13.  With the
+All loops fit the bath to a relative tolerance of 1e-13.  With the
 reference's 1e-6 the fit stops on a flat stretch of the cost before the
 parameters settle, and the loop is not reproducible to 1e-6 even against
 itself: a 1e-11 relative change of G_cl, well inside the solver's parity,
@@ -18,23 +21,80 @@ import pytest
 from test_dmft_host import oracle_solver
 
 pytestmark = pytest.mark.gpu
+TOL = 1e-6
 
 
-def test_bethe_dmft_gpu_matches_oracle(pkg, solver, configs, oracle_mod):
-    d = importlib.import_module("dmft_ed_zt_b200.dmft")
+def _dmft():
+    return importlib.import_module("dmft_ed_zt_b200.dmft")
+
+
+@pytest.fixture(scope="module")
+def bethe(pkg, configs, oracle_mod):
+    d = _dmft()
     cfg = configs.bethe_n6()
     m = cfg["model"]
     w = pkg.matsubara(cfg["nw"], cfg["beta"])
-    gpu = d.gpu_solver(pkg, solver, m.norb, m.nbath, m.U, m.Up, m.Jex, m.Jp, m.mu, cfg["sectors"], cfg["maxnstep"], w)
     cpu = oracle_solver(oracle_mod, m, cfg["sectors"], cfg["maxnstep"], w)
-    kw = dict(nloop=20, scf_tol=0.0, mixing=0.5, fit_ftol=1e-13)
-    r_gpu = d.dmft_loop(gpu, m.em, m.ek, m.vmk, w, m.nbath, **kw)
-    r_cpu = d.dmft_loop(cpu, m.em, m.ek, m.vmk, w, m.nbath, **kw)
-    assert r_gpu.iterations == r_cpu.iterations == 20
-    assert np.abs(r_gpu.D_cl - r_cpu.D_cl).max() <= 1e-6
-    assert np.abs(r_gpu.G_cl - r_cpu.G_cl).max() <= 1e-6
-    assert np.abs(r_gpu.G_loc - r_cpu.G_loc).max() <= 1e-6
-    z_gpu = d.quasiparticle_weight(d.self_energy(r_gpu.em, r_gpu.D_cl, r_gpu.G_cl, w, m.mu), w)
-    z_cpu = d.quasiparticle_weight(d.self_energy(r_cpu.em, r_cpu.D_cl, r_cpu.G_cl, w, m.mu), w)
-    assert np.abs(z_gpu - z_cpu).max() <= 1e-6
-    assert r_gpu.history[-1] < 1e-3 * r_gpu.history[0]     # the loop converges
+    ref = d.dmft_loop(cpu, m.em, m.ek, m.vmk, w, m.nbath, nloop=20, scf_tol=0.0, mixing=0.5, fit_ftol=1e-13)
+    ref1 = d.dmft_loop(cpu, m.em, m.ek, m.vmk, w, m.nbath, nloop=6, scf_tol=0.0, mixing=1.0, fit_ftol=1e-13)
+    return dict(cfg=cfg, m=m, w=w, ref=ref, ref1=ref1)
+
+
+def _z(d, r, w, mu):
+    return d.quasiparticle_weight(d.self_energy(r.em, r.D_cl, r.G_cl, w, mu), w)
+
+
+def test_bethe_dmft_python_loop_on_gpu(pkg, solver, bethe):
+    d = _dmft()
+    cfg, m, w, ref = bethe["cfg"], bethe["m"], bethe["w"], bethe["ref"]
+    gpu = d.gpu_solver(pkg, solver, m.norb, m.nbath, m.U, m.Up, m.Jex, m.Jp, m.mu, cfg["sectors"], cfg["maxnstep"], w)
+    r = d.dmft_loop(gpu, m.em, m.ek, m.vmk, w, m.nbath, nloop=20, scf_tol=0.0, mixing=0.5, fit_ftol=1e-13)
+    assert r.iterations == ref.iterations == 20
+    for a, b in ((r.D_cl, ref.D_cl), (r.G_cl, ref.G_cl), (r.G_loc, ref.G_loc)):
+        assert np.abs(a - b).max() <= TOL
+    assert np.abs(_z(d, r, w, m.mu) - _z(d, ref, w, m.mu)).max() <= TOL
+    assert r.history[-1] < 1e-3 * r.history[0]            # the loop converges
+
+
+def test_bethe_dmft_library_loop(pkg, solver, bethe, tmp_path):
+    d = _dmft()
+    cfg, m, w, ref = bethe["cfg"], bethe["m"], bethe["w"], bethe["ref"]
+    r = solver.dmft_bethe(m, cfg["sectors"], cfg["maxnstep"], w, nspin=1, nloop=20, scf_tol=0.0, mixing=0.5,
+                          fit_ftol=1e-13, outdir=str(tmp_path))
+    assert r["iterations"] == 20 and not r["converged"] and len(r["history"]) == 20
+    for key in ("D_cl", "G_cl", "G_loc"):
+        assert np.abs(r[key] - getattr(ref, key)).max() <= TOL, key
+    assert np.abs(r["em"] - ref.em).max() <= 1e-4               # the bath itself is only loosely fixed
+    assert np.abs(r["Z"] - _z(d, ref, w, m.mu)).max() <= TOL
+    assert np.abs(np.array(r["history"]) - np.array(ref.history)).max() <= 1e-6 * max(ref.history)
+    # the reference's files, written every iteration (the last one stays)
+    rows = open(tmp_path / "green.dat.1.1").read().split("\n")
+    assert rows[0].split() == ["2048", "1", "1"] and len(rows[1]) == 7 * 12
+    g = np.array([[float(row[12 * k:12 * (k + 1)]) for k in range(7)] for row in rows[1:3]])
+    assert np.abs(g[:, 3] + 1j * g[:, 4] - r["G_cl"][0, 0, :2]).max() <= 1e-8
+    vals = open(tmp_path / "h_imp.dat").read().split()
+    assert vals[:3] == ["1", "5", "1"] and len(vals) == 3 + 1 + 5 + 5
+    assert np.allclose([float(v) for v in vals[4:9]], r["ek"][:, 0], rtol=0, atol=1e-15)
+    co = open(tmp_path / "g_coeffs.dat").read().split("\n")
+    assert co[0].split() == ["200", "1"] and co[1].split()[:2] == ["1", "1"] and len(co[2].split()) == 4
+    assert co[202].split()[:2] == ["1", "2"]                   # spin 2 block (spin-even: the same coefficients)
+    assert co[2] == co[203]
+    assert open(tmp_path / "sigma.dat.1.1").read().split("\n")[0].split() == ["2048", "1", "1"]
+
+
+def test_bethe_dmft_library_loop_without_mixing(pkg, solver, bethe):
+    cfg, m, w, ref1 = bethe["cfg"], bethe["m"], bethe["w"], bethe["ref1"]
+    r = solver.dmft_bethe(m, cfg["sectors"], cfg["maxnstep"], w, nspin=1, nloop=6, scf_tol=0.0, mixing=1.0,
+                          fit_ftol=1e-13)
+    assert r["iterations"] == 6
+    for key in ("D_cl", "G_cl", "G_loc"):
+        assert np.abs(r[key] - getattr(ref1, key)).max() <= TOL, key
+
+
+def test_bethe_dmft_library_loop_stops_and_rejects(pkg, solver, bethe):
+    cfg, m, w = bethe["cfg"], bethe["m"], bethe["w"]
+    r = solver.dmft_bethe(m, cfg["sectors"], cfg["maxnstep"], w[:256], nloop=20, scf_tol=1e-3)
+    assert r["converged"] and r["iterations"] < 20 and r["history"][-1] < 1e-3
+    with pytest.raises(pkg.EDError) as e:
+        solver.dmft_bethe(m, cfg["sectors"], cfg["maxnstep"], w, mixing=0.0)
+    assert e.value.code == pkg.EDZT_ERR_ARG
