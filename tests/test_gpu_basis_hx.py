@@ -120,6 +120,35 @@ def test_hx_large_rows_and_hermiticity(pkg, solver, oracle_mod, nsite):
         assert np.abs(yh[r0:r1] - ref).max() <= _tol(ref)
 
 
+@pytest.mark.parametrize("norb,nbath,J,sector", [(1, 5, 0.0, (3, 3)), (1, 5, 0.0, (2, 4)), (2, 4, 0.6, (3, 3)),
+                                                 (3, 3, 0.4, (3, 2))])
+def test_hx_matrix_elements_bit_exact(pkg, solver, oracle_mod, norb, nbath, J, sector):
+    """Every (ket index, sign) of the GPU's hop tables, bit for bit: column j
+    of H is H e_j, and each off-diagonal element is one product (+-V or
+    +-Jp) times 1.0, so the GPU's and the oracle's dense H must agree exactly
+    off the diagonal.  The diagonal sums several terms (ulp-level bound)."""
+    import torch
+    rng = np.random.default_rng(40 + norb)
+    m = random_model(pkg, rng, norb, nbath, J=J, spin_dep=True)
+    solver.set_model(m)
+    o = oracle_for(oracle_mod, m)
+    nu, nd = sector
+    H_ref = o.dense_h(nu, nd)
+    n = H_ref.shape[0]
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    H = np.zeros((n, n))
+    for j in range(n):
+        x.zero_()
+        x[j] = 1.0
+        solver.hx(nu, nd, x, y)
+        H[:, j] = y.cpu().numpy()
+    off = ~np.eye(n, dtype=bool)
+    assert np.array_equal(H[off], H_ref[off])
+    assert np.count_nonzero(H_ref[off]) > 0
+    assert np.abs(np.diag(H) - np.diag(H_ref)).max() <= 1e-14 * np.abs(np.diag(H_ref)).max()
+
+
 def test_hx_device_pointers_accumulate(pkg, solver, oracle_mod):
     import torch
     rng = np.random.default_rng(9)
