@@ -198,16 +198,17 @@ def batched_leg(pkg, s, cfgs, n):
             "sample": f"first {n} of the 256 seeded instances (seed 4), wall clock of one call, synchronised"}
 
 
-def served_leg(pkg, s, cfgs, n, seed=5):
+def served_leg(pkg, s, cfgs, n, seed=5, nsite_max=12):
     """The served form: n requests with Poisson arrivals (mean 200 req/s),
-    nsite ~ U{8..12}, random U, J = 0, bath as the batched form, nspin 2,
-    through edzt_server's request loop."""
+    nsite ~ U{8..nsite_max} (the workload's distribution is U{8..16}; the
+    default run stops at 12 to stay within minutes), random U, J = 0, bath as
+    the batched form, nspin 2, through edzt_server's request loop."""
     import numpy as np
     rng = np.random.default_rng(seed)
     omega = pkg.matsubara(2048, 100.0)
     reqs = []
     for _ in range(n):
-        ns = int(rng.integers(8, 13))
+        ns = int(rng.integers(8, nsite_max + 1))
         nb = ns - 1
         U = float(rng.uniform(1.0, 4.0))
         ek = rng.uniform(-2.0, 2.0, nb)
@@ -231,8 +232,10 @@ def served_leg(pkg, s, cfgs, n, seed=5):
             "offered_rate_per_s": 200.0,
             "plain_gpu": {"value": plain, "unit": "solves/s", "ms_per_solve_by_nsite": per_ns,
                           "how": "one request per nsite timed, weighted by counts"},
-            "sample": f"{n} requests, nsite 8..12 of the 8..16 distribution (nsite 13..16 solves take seconds "
-                      "each and do not fit the bench's time bound), Poisson 200/s (seed 5)"}
+            "sample": (f"{n} requests, nsite 8..{nsite_max}" +
+                       (" of the 8..16 distribution (nsite 13..16 solves take seconds each and do not fit the "
+                        "default run's time bound; --served-nsite-max 16 runs all)" if nsite_max < 16 else "") +
+                       ", Poisson 200/s (seed 5)")}
 
 
 def hv_leg(pkg, s, peak):
@@ -484,7 +487,7 @@ def run_gpu(args):
         batched = batched_leg(pkg, s, cfgs, args.batched)
     if world == 1 and args.served > 0:
         cfgs = importlib.import_module("dmft_ed_zt_b200.configs")
-        served = served_leg(pkg, s, cfgs, args.served)
+        served = served_leg(pkg, s, cfgs, args.served, nsite_max=args.served_nsite_max)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -579,6 +582,8 @@ def main():
     ap.add_argument("--skip-hv", action="store_true")
     ap.add_argument("--batched", type=int, default=64, help="instances of the batched leg (0: skip)")
     ap.add_argument("--served", type=int, default=32, help="requests of the served leg (0: skip)")
+    ap.add_argument("--served-nsite-max", type=int, default=12, choices=range(8, 17),
+                    help="largest nsite of the served leg's requests (the workload's is 16)")
     ap.add_argument("--traffic-file", default=os.path.join(ROOT, "profiles", "k_lanczos_aim_n12_dram.txt"))
     ap.add_argument("--case", default=None, help="run one small profiling case (hx:NS, lz:NS, solve) and exit")
     args = ap.parse_args()
