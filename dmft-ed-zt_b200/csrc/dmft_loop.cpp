@@ -36,6 +36,9 @@
 #include <vector>
 #include "../../include/edzt.h"
 
+// The context's error message (edzt_last_error), set by the library's host code.
+void edzt_ctx_set_error(edzt_ctx* c, const char* msg);
+
 namespace {
 
 using cplx = std::complex<double>;
@@ -44,6 +47,7 @@ constexpr double kGold = 1.618034, kCGold = 0.3819660, kGLimit = 100.0, kTiny = 
 
 struct Fail {
     int code;
+    const char* msg;   // nullptr: the solver call already set the context's message
 };
 
 size_t gidx(int iw, int a, int s, int nw, int norb) { return (size_t)iw + (size_t)nw * ((size_t)a + (size_t)norb * s); }
@@ -252,7 +256,7 @@ double brent(F& f, double ax, double bx, double cx, double& xmin, double tol = 1
             else if (fu <= fv || v == x || v == w) { v = u; fv = fu; }
         }
     }
-    throw Fail{EDZT_ERR_NUMERIC};
+    throw Fail{EDZT_ERR_NUMERIC, "bath fit: line minimisation did not converge"};
 }
 
 // Polak-Ribiere conjugate gradient with exact line searches; stops when a
@@ -285,7 +289,7 @@ double conjugate_gradient(const BathFit& bf, std::vector<double>& p, double ftol
         const double gam = dgg / gg;
         for (size_t i = 0; i < n; i++) { g[i] = -xi[i]; h[i] = g[i] + gam * h[i]; xi[i] = h[i]; }
     }
-    throw Fail{EDZT_ERR_NUMERIC};
+    throw Fail{EDZT_ERR_NUMERIC, "bath fit: conjugate gradient did not converge"};
 }
 
 // New (em, ek, vmk), fitted per spin; with nspin 1 spin down copies spin up.
@@ -322,7 +326,7 @@ void write_h_imp(const char* dir, int norb, int nbath, int nspin, const double* 
                  const double* vmk)
 {
     FILE* f = std::fopen(path_in(dir, "h_imp.dat").c_str(), "w");
-    if (!f) throw Fail{EDZT_ERR_ARG};
+    if (!f) throw Fail{EDZT_ERR_ARG, "cannot write an output file in outdir"};
     std::fprintf(f, " %11d %11d %11d\n", norb, nbath, nspin);
     for (int s = 0; s < nspin; s++) {
         for (int a = 0; a < norb; a++) std::fprintf(f, " %25.16E\n", em[a + norb * s]);
@@ -342,7 +346,7 @@ void write_functions(const char* dir, const char* stem, int norb, int nspin, int
         for (int a = 0; a < norb; a++) {
             const std::string name = std::string(stem) + "." + std::to_string(a + 1) + "." + std::to_string(s + 1);
             FILE* f = std::fopen(path_in(dir, name).c_str(), "w");
-            if (!f) throw Fail{EDZT_ERR_ARG};
+            if (!f) throw Fail{EDZT_ERR_ARG, "cannot write an output file in outdir"};
             std::fprintf(f, " %11d %11d %11d\n", nw, a + 1, s + 1);
             for (int w = 0; w < nw; w++) {
                 std::fprintf(f, "%12.8f", omega[w]);
@@ -362,7 +366,7 @@ void write_functions(const char* dir, const char* stem, int norb, int nspin, int
 void write_g_coeffs(const char* dir, int norb, int maxnstep, double e0, const double* coeffs)
 {
     FILE* f = std::fopen(path_in(dir, "g_coeffs.dat").c_str(), "w");
-    if (!f) throw Fail{EDZT_ERR_ARG};
+    if (!f) throw Fail{EDZT_ERR_ARG, "cannot write an output file in outdir"};
     std::fprintf(f, " %11d %11d\n", maxnstep, norb);
     for (int a = 0; a < norb; a++)
         for (int s = 0; s < 2; s++) {
@@ -426,8 +430,11 @@ int edzt_dmft_bethe(edzt_ctx* ctx, const edzt_dmft_params* p, double* em, double
     const int norb = p->norb, nbath = p->nbath, nspin = p->nspin, nw = p->nw;
     if (norb < 1 || nbath < 1 || (nspin != 1 && nspin != 2) || nw < 1 || !p->omega || p->nloop < 1 ||
         p->nsector < 1 || !p->sectors || p->maxnstep < 1 || !(p->mixing > 0.0 && p->mixing <= 1.0) ||
-        !(p->fit_ftol > 0.0) || !finite_all(p->omega, nw))
+        !(p->fit_ftol > 0.0) || !finite_all(p->omega, nw)) {
+        edzt_ctx_set_error(ctx, "edzt_dmft_bethe: invalid parameters (sizes, sectors, nloop, mixing in (0, 1], "
+                                "fit_ftol > 0, finite omega)");
         return EDZT_ERR_ARG;
+    }
     const size_t ng = (size_t)nw * norb * nspin;
     std::vector<cplx> D(ng), Gc(ng), Gl(ng);
     std::vector<double> coeffs((size_t)norb * 2 * 4 * p->maxnstep);
@@ -448,15 +455,15 @@ int edzt_dmft_bethe(edzt_ctx* ctx, const edzt_dmft_params* p, double* em, double
             }
             hybridization(norb, nbath, nspin, nw, p->omega, ek, vmk, D.data());
             if ((rc = edzt_set_model(ctx, norb, nbath, em, ek, vmk, p->U, p->Up, p->Jex, p->Jp, p->mu)) != EDZT_OK)
-                throw Fail{rc};
+                throw Fail{rc, nullptr};
             int isector = 0;
             double e0 = 0.0;
             if ((rc = edzt_ground_state(ctx, p->nsector, p->sectors, p->maxnstep, p->seed, &isector, &e0, nullptr,
                                         nullptr)) != EDZT_OK)
-                throw Fail{rc};
+                throw Fail{rc, nullptr};
             if ((rc = edzt_cluster_green_ftn(ctx, nspin, p->maxnstep, nw, p->omega, reinterpret_cast<double*>(Gc.data()),
                                              coeffs.data())) != EDZT_OK)
-                throw Fail{rc};
+                throw Fail{rc, nullptr};
             local_green(norb, nspin, nw, em, p->hfield, D.data(), Gc.data(), Gl.data());
             if (p->outdir) {                                      // dump_data every iteration (dmft.f90:82)
                 write_h_imp(p->outdir, norb, nbath, nspin, em, ek, vmk);
@@ -482,6 +489,7 @@ int edzt_dmft_bethe(edzt_ctx* ctx, const edzt_dmft_params* p, double* em, double
                     Z[a + norb * s] = 1.0 / (1.0 - S[gidx(0, a, s, nw, norb)].imag() / p->omega[0]);
         if (p->outdir) write_functions(p->outdir, "sigma.dat", norb, nspin, nw, p->omega, {S.data()});
     } catch (const Fail& e) {
+        if (e.msg) edzt_ctx_set_error(ctx, e.msg);
         return e.code;
     }
     if (D_cl) std::copy(D.begin(), D.end(), reinterpret_cast<cplx*>(D_cl));

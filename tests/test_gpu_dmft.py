@@ -97,4 +97,7 @@ def test_bethe_dmft_library_loop_stops_and_rejects(pkg, solver, bethe):
     assert r["converged"] and r["iterations"] < 20 and r["history"][-1] < 1e-3
     with pytest.raises(pkg.EDError) as e:
         solver.dmft_bethe(m, cfg["sectors"], cfg["maxnstep"], w, mixing=0.0)
-    assert e.value.code == pkg.EDZT_ERR_ARG
+    assert e.value.code == pkg.EDZT_ERR_ARG and "mixing" in str(e.value)
+    with pytest.raises(pkg.EDError) as e:
+        solver.dmft_bethe(m, cfg["sectors"], cfg["maxnstep"], w[:64], nloop=1, outdir="/nonexistent/dmft/run")
+    assert e.value.code == pkg.EDZT_ERR_ARG and "outdir" in str(e.value)
