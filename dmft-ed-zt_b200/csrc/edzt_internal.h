@@ -1,6 +1,7 @@
 // edzt_internal.h — host-side declarations shared by the CUDA translation
 // units of libedzt (not part of the public C ABI; see include/edzt.h).
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "edzt_device.cuh"
@@ -15,6 +16,17 @@ struct DevModel {
     double vmk[EDZT_MAX_NORB][EDZT_MAX_NSITE][2];
     double U, Up, Jex, Jp, mu;
 };
+
+// True the first time it is called for the current device with this set of
+// flags: per-device one-time set-up such as a kernel's shared-memory
+// attribute, which cudaFuncSetAttribute sets for the current device only.
+inline bool edzt_once_per_device(std::atomic<unsigned long long>& done)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    const unsigned long long bit = 1ull << dev;
+    return (done.fetch_or(bit) & bit) == 0;
+}
 
 // ---- tables.cu -------------------------------------------------------------
 void edzt_init_binomials(int device);

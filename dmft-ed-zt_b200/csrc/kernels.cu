@@ -84,11 +84,10 @@ template <int T>
 static void launch_hx_t(const DevSector& S, const double* x, double* y, int accumulate, int tiles, int R,
                         size_t smem, cudaStream_t s)
 {
-    static bool attr_set = false;
-    if (!attr_set) {
+    static std::atomic<unsigned long long> attr_set{0};
+    if (edzt_once_per_device(attr_set)) {
         cudaFuncSetAttribute(k_hx<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         cudaFuncSetAttribute(k_hx<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr_set = true;
     }
     if (accumulate) k_hx<true, T><<<tiles, T, smem, s>>>(S, x, y, R);
     else k_hx<false, T><<<tiles, T, smem, s>>>(S, x, y, R);

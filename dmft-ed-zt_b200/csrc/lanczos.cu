@@ -493,11 +493,9 @@ int lz_debug_bad(long long* out4)
 
 int lz_grid_size(int device, size_t smem, int* block_out)
 {
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (edzt_once_per_device(attr))
         cudaFuncSetAttribute(k_lanczos, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr = true;
-    }
     int per_sm = 0, nsm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos, kLzThreads, smem);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
