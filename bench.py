@@ -357,7 +357,10 @@ def run_gpu(args):
                                 device_id=torch.device("cuda", local))
 
     pkg = load_pkg()
-    pkg.build()
+    if local == 0:                       # one make per node; the other ranks wait for it
+        pkg.build()
+    if dist is not None:
+        dist.barrier()
     cfg = workload()
     m = cfg["model"]
     sectors = cfg["sectors"]
