@@ -3,9 +3,10 @@
  *
  * Drop-in boundary for the hot path of yw-choi/DMFT-ED-ZT.  Each entry point
  * replaces one Fortran procedure of the reference (cited per function); a
- * Fortran host binds them through iso_c_binding (INTEGRATION.md gives the
- * interface module).  The DMFT loop, lattice, grid and bath fit stay on the
- * host unchanged.
+ * Fortran host binds them through an iso_c_binding interface module with
+ * one bind(C) interface per function.  The reference's DMFT loop, lattice,
+ * grid and bath fit can stay on the host unchanged; the library also
+ * carries a Bethe-lattice DMFT loop of its own (edzt_dmft_bethe).
  *
  * Conventions
  *  - Every function returns EDZT_OK (0) or an error code; edzt_last_error()
