@@ -127,3 +127,24 @@ def test_library_host_loop_pieces_match_restatement(pkg, oracle_mod):
             assert np.abs(d.hybridization(got[1], got[2], w, nspin) - D).max() <= 1e-5
     with pytest.raises(pkg.EDError):
         pkg.fit_bath(em, ek, V, D, G_cl, G_loc, w, nspin, ftol=0.0)
+
+
+def _dmft_golden():
+    import importlib.util
+    import os
+    from conftest import ROOT
+    path = os.path.join(ROOT, "tests", "golden", "make_dmft_golden.py")
+    spec = importlib.util.spec_from_file_location("make_dmft_golden", path)
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    return gen, np.load(gen.OUT)
+
+
+def test_dmft_loop_reproduces_golden(pkg):
+    """The Python DMFT loop on the oracle reproduces the committed record of
+    a short run (tests/golden/make_dmft_golden.py) within the DMFT bound."""
+    gen, gold = _dmft_golden()
+    _, r = gen.run_oracle_loop()
+    for key in ("D_cl", "G_cl", "G_loc", "em", "ek"):
+        assert np.abs(getattr(r, key) - gold[key]).max() <= 1e-6, key
+    assert np.allclose(r.history, gold["history"], rtol=1e-4, atol=0)
