@@ -9,7 +9,9 @@
 //   iteration > 1: fit (em, ek, vmk) to the previous iteration's G_0^-1
 //                  corrected by G_loc^-1 - G_cl^-1 (src/ed_projection.f90:23-553),
 //                  optionally mixed linearly with the previous parameters
-//                  (mixing 1 reproduces the reference, which has no mixing)
+//                  after aligning the fitted bath sites' signs with the
+//                  previous ones (mixing 1 reproduces the reference, which
+//                  has no mixing)
 //   then           D_cl  = sum_l V_l^2 / (i w - e_l)             (dmft_green.f90:24-45)
 //                  G_cl  = edzt_ground_state + edzt_cluster_green_ftn
 //                  G_loc = int dos(x) / (em + D_cl + 1/G_cl - x) dx  (dmft_green.f90:128-170)
@@ -319,6 +321,22 @@ void fit_bath(int norb, int nbath, int nspin, int nw, const double* omega, doubl
     }
 }
 
+// Each fitted bath site's couplings (the column vmk(:, l, s)) take the sign
+// that best matches the previous ones.  The fit's cost depends on them only
+// through products V_a V_b of one site, so a site's overall sign is free and
+// the conjugate gradient may return either; linear mixing of vmk is only
+// meaningful between columns of the same sign.
+void align_bath_signs(int norb, int nbath, double* vmk_new, const double* vmk_old)
+{
+    for (int s = 0; s < 2; s++)
+        for (int l = 0; l < nbath; l++) {
+            double dot = 0.0;
+            for (int a = 0; a < norb; a++) dot += vmk_new[a + norb * (l + nbath * s)] * vmk_old[a + norb * (l + nbath * s)];
+            if (dot < 0.0)
+                for (int a = 0; a < norb; a++) vmk_new[a + norb * (l + nbath * s)] = -vmk_new[a + norb * (l + nbath * s)];
+        }
+}
+
 // ---- the reference's output files ------------------------------------------
 std::string path_in(const char* dir, const std::string& name) { return std::string(dir) + "/" + name; }
 
@@ -449,6 +467,7 @@ int edzt_dmft_bethe(edzt_ctx* ctx, const edzt_dmft_params* p, double* em, double
                 fit_bath(norb, nbath, nspin, nw, p->omega, emf.data(), ekf.data(), vmf.data(), D.data(), Gc.data(),
                          Gl.data(), p->fit_ftol, nullptr);
                 const double m = p->mixing;
+                if (m < 1.0) align_bath_signs(norb, nbath, vmf.data(), vmk);
                 for (int i = 0; i < 2 * norb; i++) em[i] = m * emf[i] + (1.0 - m) * em[i];
                 for (int i = 0; i < 2 * nbath; i++) ek[i] = m * ekf[i] + (1.0 - m) * ek[i];
                 for (size_t i = 0; i < 2 * (size_t)norb * nbath; i++) vmk[i] = m * vmf[i] + (1.0 - m) * vmk[i];

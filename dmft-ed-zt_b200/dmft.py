@@ -290,11 +290,28 @@ class DMFTResult:
     history: list = field(default_factory=list)
 
 
+def align_bath_signs(vmk_new, vmk_old):
+    """vmk_new with each bath site's couplings (the column vmk[:, l, s]) given
+    the sign that best matches vmk_old.  The fit's cost depends on the
+    couplings only through products V_a V_b of one site, so a site's overall
+    sign is free and the conjugate gradient may return either; linear mixing
+    of vmk is only meaningful between columns of the same sign."""
+    v = np.array(vmk_new, dtype=float, copy=True)
+    old = np.asarray(vmk_old, dtype=float)
+    for s in range(v.shape[2]):
+        for l in range(v.shape[1]):
+            if float(v[:, l, s] @ old[:, l, s]) < 0.0:
+                v[:, l, s] = -v[:, l, s]
+    return v
+
+
 def dmft_loop(solve, em, ek, vmk, omega, nbath, nspin=1, nloop=20, scf_tol=1.0e-6, mixing=1.0, hfield=0.0,
               writer=None, fit_ftol=1.0e-6):
     """The DMFT iterations of dmft.f90:55-98 with `solve(em, ek, vmk)` ->
     G_cl[ispin, iorb, iw] as the impurity solver.  mixing mixes the fitted
-    parameters with the previous ones (1: the reference's loop).
+    parameters with the previous ones (1: the reference's loop); before a
+    mixing below 1 the fitted bath sites take the signs of the previous ones
+    (align_bath_signs).
 
     fit_ftol is the bath fit's stopping tolerance.  At the reference's 1e-6
     the fit stops where the cost is flat but the parameters are not settled,
@@ -310,6 +327,8 @@ def dmft_loop(solve, em, ek, vmk, omega, nbath, nspin=1, nloop=20, scf_tol=1.0e-
     for it in range(1, nloop + 1):
         if it > 1:
             em_f, ek_f, vmk_f, info = fit_bath(em, ek, vmk, D, G_cl, G_loc, omega, nspin, fit_ftol)
+            if mixing < 1.0:
+                vmk_f = align_bath_signs(vmk_f, vmk)
             em = mixing * em_f + (1.0 - mixing) * em
             ek = mixing * ek_f + (1.0 - mixing) * ek
             vmk = mixing * vmk_f + (1.0 - mixing) * vmk

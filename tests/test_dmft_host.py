@@ -148,3 +148,16 @@ def test_dmft_loop_reproduces_golden(pkg):
     for key in ("D_cl", "G_cl", "G_loc", "em", "ek"):
         assert np.abs(getattr(r, key) - gold[key]).max() <= 1e-6, key
     assert np.allclose(r.history, gold["history"], rtol=1e-4, atol=0)
+
+
+def test_bath_sign_alignment(pkg):
+    """Before mixing, each fitted bath site keeps the overall sign of its
+    previous couplings: the fit's cost is blind to it (only V_a V_b of a site
+    enter), and mixing columns of opposite sign would shrink the bath."""
+    d = _dmft(pkg)
+    old = np.array([[[0.5, 0.5], [0.3, 0.3], [-0.2, -0.2]],
+                    [[0.1, 0.1], [-0.4, -0.4], [0.6, 0.6]]])          # (norb 2, nbath 3, spin 2)
+    new = old * np.array([-1.0, 1.0, -1.0])[None, :, None] * 1.1
+    got = d.align_bath_signs(new, old)
+    assert np.allclose(got, old * 1.1)
+    assert np.array_equal(d.align_bath_signs(old, old), old)
