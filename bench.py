@@ -195,7 +195,8 @@ def batched_leg(pkg, s, cfgs, n):
             "nsite_counts_8_to_14": hist, "plain_gpu": {"value": plain, "unit": "solves/s",
                                                         "ms_per_solve_by_nsite": per_ns,
                                                         "how": "one instance per nsite timed, weighted by counts"},
-            "sample": f"first {n} of the 256 seeded instances (seed 4), wall clock of one call, synchronised"}
+            "sample": (f"all 256 seeded instances (seed 4)" if n >= 256 else
+                       f"first {n} of the 256 seeded instances (seed 4)") + ", wall clock of one call, synchronised"}
 
 
 def served_leg(pkg, s, cfgs, n, seed=5, nsite_max=12):
@@ -601,7 +602,7 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-hv", action="store_true")
-    ap.add_argument("--batched", type=int, default=64, help="instances of the batched leg (0: skip)")
+    ap.add_argument("--batched", type=int, default=256, help="instances of the batched leg (0: skip)")
     ap.add_argument("--served", type=int, default=32, help="requests of the served leg (0: skip)")
     ap.add_argument("--served-nsite-max", type=int, default=12, choices=range(8, 17),
                     help="largest nsite of the served leg's requests (the workload's is 16)")
