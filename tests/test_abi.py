@@ -50,3 +50,27 @@ def test_model_defaults(pkg):
     assert m.Up == 1.0 and m.Jp == 0.5          # src/dmft_params.f90:90-96
     w = pkg.matsubara(3, np.pi)
     assert np.allclose(w, [1.0, 3.0, 5.0])
+
+
+def test_struct_layouts_match_python_mirror(pkg, tmp_path):
+    """The ctypes mirrors of edzt_instance and edzt_dmft_params have the C
+    layout: sizes and every field offset, from a C program built against
+    include/edzt.h with the host compiler."""
+    import subprocess
+    structs = {"edzt_instance": pkg.Instance, "edzt_dmft_params": pkg.DMFTParams}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "edzt.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
