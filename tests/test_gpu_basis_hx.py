@@ -90,7 +90,8 @@ def test_hx_kanamori_full(solver, configs, oracle_mod):
 @pytest.mark.parametrize("nsite", [14, 15, 16])
 def test_hx_large_rows_and_hermiticity(pkg, solver, oracle_mod, nsite):
     """Full-size sectors: oracle rows at three offsets, <u,Hv> = <Hu,v> on the
-    device.  They run k_hx with 512 (nsite 14) and 1024 threads per CTA
+    device, for y = H x and y += H x.  They run k_hx with 512 threads per
+    CTA (nsite 14) and its persistent double-buffered form with 1024
     (nsite 15 and 16)."""
     import torch
     rng = np.random.default_rng(nsite)
@@ -112,6 +113,10 @@ def test_hx_large_rows_and_hermiticity(pkg, solver, oracle_mod, nsite):
     rhs = float(torch.dot(hu, x))
     scale = float(torch.linalg.norm(u) * torch.linalg.norm(y))
     assert abs(lhs - rhs) <= 1e-11 * scale
+    z = u.clone()                                           # the accumulating form: z = u + H x
+    solver.hx(nu, nd, x, z, py=True)
+    torch.cuda.synchronize()
+    assert float((z - u - y).abs().max()) <= 1e-13 * (float(y.abs().max()) + float(u.abs().max()) + 1.0)
     xh = x.cpu().numpy()
     yh = y.cpu().numpy()
     for r0 in (0, n // 2 - 20000, n - 40000):
