@@ -90,9 +90,8 @@ def test_hx_kanamori_full(solver, configs, oracle_mod):
 @pytest.mark.parametrize("nsite", [14, 15, 16])
 def test_hx_large_rows_and_hermiticity(pkg, solver, oracle_mod, nsite):
     """Full-size sectors: oracle rows at three offsets, <u,Hv> = <Hu,v> on the
-    device, for y = H x and y += H x.  They run k_hx with 512 threads per
-    CTA (nsite 14) and its persistent double-buffered form with 1024
-    (nsite 15 and 16)."""
+    device, for y = H x and y += H x.  They run k_hx with 512 (nsite 14)
+    and 1024 threads per CTA (nsite 15 and 16)."""
     import torch
     rng = np.random.default_rng(nsite)
     m = random_model(pkg, rng, 1, nsite - 1)
