@@ -124,8 +124,23 @@ def test_hx_large_rows_and_hermiticity(pkg, solver, oracle_mod, nsite):
         assert np.abs(yh[r0:r1] - ref).max() <= _tol(ref)
 
 
+def _random_element_cases(n=6, seed=77, max_dim=600):
+    """Seeded random (norb, nbath, J, sector) with sector dimension <= max_dim."""
+    from math import comb
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < n:
+        norb = int(rng.integers(1, 4))
+        nbath = int(rng.integers(1, 8 - norb))
+        ns = norb + nbath
+        nu, nd = int(rng.integers(0, ns + 1)), int(rng.integers(0, ns + 1))
+        if 2 <= comb(ns, nu) * comb(ns, nd) <= max_dim:
+            out.append((norb, nbath, float(rng.uniform(0.0, 0.8)) if norb > 1 else 0.0, (nu, nd)))
+    return out
+
+
 @pytest.mark.parametrize("norb,nbath,J,sector", [(1, 5, 0.0, (3, 3)), (1, 5, 0.0, (2, 4)), (2, 4, 0.6, (3, 3)),
-                                                 (3, 3, 0.4, (3, 2))])
+                                                 (3, 3, 0.4, (3, 2))] + _random_element_cases())
 def test_hx_matrix_elements_bit_exact(pkg, solver, oracle_mod, norb, nbath, J, sector):
     """Every (ket index, sign) of the GPU's hop tables, bit for bit: column j
     of H is H e_j, and each off-diagonal element is one product (+-V or
