@@ -96,12 +96,51 @@ class EDError(RuntimeError):
         self.code = code
 
 
-def build(force: bool = False) -> str:
-    """Compile libedzt.so for sm_100a with nvcc (cross-compiles without a GPU)."""
+STAMP_PATH = LIB_PATH + ".stamp"
+
+
+def source_hash() -> str:
+    """SHA-256 over the library's sources: the Makefile, csrc/ and the C ABI
+    header, in sorted path order."""
+    import hashlib
+    h = hashlib.sha256()
+    files = [os.path.join(PKG_DIR, "Makefile"), os.path.join(REPO_ROOT, "include", "edzt.h")]
+    csrc = os.path.join(PKG_DIR, "csrc")
+    files += sorted(os.path.join(csrc, f) for f in os.listdir(csrc))
+    for f in files:
+        h.update(os.path.relpath(f, REPO_ROOT).encode() + b"\0")
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()
+
+
+def build(force: bool = False, verbose: bool = True) -> str:
+    """Compile libedzt.so for sm_100a with nvcc (cross-compiles without a GPU).
+
+    The library is rebuilt from scratch whenever the hash of its sources
+    differs from the stamp written beside it by the last build (or either is
+    missing), so a shipped library is reused only if it was built from these
+    exact sources.  Logs which of the two happened on stderr."""
+    import sys
     if os.environ.get("EDZT_LIBRARY"):
         return LIB_PATH
-    args = ["make", "-s", "-C", PKG_DIR, "-j4"] + (["-B"] if force else []) + ["libedzt.so"]
-    subprocess.run(args, check=True)
+    want = source_hash()
+    try:
+        with open(STAMP_PATH) as f:
+            have = f.read().strip()
+    except OSError:
+        have = ""
+    if not force and have == want and os.path.exists(LIB_PATH):
+        if verbose:
+            print(f"libedzt: reusing {os.path.basename(LIB_PATH)} built from sources {want[:16]}", file=sys.stderr)
+        return LIB_PATH
+    if os.path.exists(STAMP_PATH):
+        os.remove(STAMP_PATH)
+    subprocess.run(["make", "-s", "-C", PKG_DIR, "-j8", "-B", "libedzt.so"], check=True)
+    with open(STAMP_PATH, "w") as f:
+        f.write(want + "\n")
+    if verbose:
+        print(f"libedzt: rebuilt from sources {want[:16]} (stamp was {have[:16] or 'missing'})", file=sys.stderr)
     return LIB_PATH
 
 

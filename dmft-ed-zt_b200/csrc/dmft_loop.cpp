@@ -20,12 +20,12 @@
 //   after the loop Sigma = i w + mu - em - D_cl - 1/G_cl, Z = 1/(1 - Im Sigma(i w_1)/w_1),
 //                  sigma.dat.<o>.<s>                              (post_process.f90:39-57, :121-185)
 //
-// The bath fit minimises the reference's cost with the reference's method:
-// the Polak-Ribiere conjugate gradient with line minimisation by golden-ratio
-// bracketing and Brent's parabolic interpolation (Press et al., Numerical
-// Recipes, 2nd ed., sections 10.1, 10.2, 10.6; R. Brent, Algorithms for
-// Minimization without Derivatives, 1973), written here from those published
-// algorithms, with the reference's tolerances (ftol 1e-6, line tolerance 1e-8).
+// The bath fit minimises the reference's cost (src/ed_projection.f90:154-250)
+// by a nonlinear conjugate gradient with Polak-Ribiere directions, as the
+// reference does, with a line search of this file's own design that uses the
+// cost's analytic gradient (fourfold step growth to a bracket, then
+// safeguarded Hermite-cubic steps) and the reference's relative stopping
+// tolerance (ftol 1e-6 by default).
 //
 // Array layouts are the reference's Fortran ones: em(norb,2), ek(nbath,2),
 // vmk(norb,nbath,2) column-major; complex functions (nw, norb, nspin)
@@ -44,8 +44,6 @@ void edzt_ctx_set_error(edzt_ctx* c, const char* msg);
 namespace {
 
 using cplx = std::complex<double>;
-
-constexpr double kGold = 1.618034, kCGold = 0.3819660, kGLimit = 100.0, kTiny = 1.0e-20, kZeps = 1.0e-10;
 
 struct Fail {
     int code;
@@ -177,119 +175,124 @@ struct BathFit {
     }
 };
 
-// Bracket a minimum of f from ax, bx: golden-ratio steps with parabolic
-// extrapolation limited to kGLimit times the last step.
-template <class F>
-void bracket(F& f, double& ax, double& bx, double& cx)
+// Minimiser of the cubic that matches value and slope at both ends of
+// [lo, hi] (Hermite interpolation); NaN when that cubic has no interior minimum.
+double cubic_step(double lo, double flo, double slo, double hi, double fhi, double shi)
 {
-    double fa = f(ax), fb = f(bx);
-    if (fb > fa) { std::swap(ax, bx); std::swap(fa, fb); }
-    cx = bx + kGold * (bx - ax);
-    double fc = f(cx);
-    while (fb > fc) {
-        const double r = (bx - ax) * (fb - fc), q = (bx - cx) * (fb - fa);
-        const double den = 2.0 * std::copysign(std::max(std::fabs(q - r), kTiny), q - r);
-        double u = bx - ((bx - cx) * q - (bx - ax) * r) / den, fu;
-        const double ulim = bx + kGLimit * (cx - bx);
-        if ((bx - u) * (u - cx) > 0.0) {                 // parabolic point between b and c
-            fu = f(u);
-            if (fu < fc) { ax = bx; bx = u; return; }
-            if (fu > fb) { cx = u; return; }
-            u = cx + kGold * (cx - bx);
-            fu = f(u);
-        } else if ((cx - u) * (u - ulim) > 0.0) {        // between c and its limit
-            fu = f(u);
-            if (fu < fc) {
-                const double un = u + kGold * (u - cx);
-                bx = cx; cx = u; u = un;
-                fb = fc; fc = fu; fu = f(u);
-            }
-        } else if ((u - ulim) * (ulim - cx) >= 0.0) {    // limited to its maximum
-            u = ulim;
-            fu = f(u);
-        } else {                                         // rejected: golden step
-            u = cx + kGold * (cx - bx);
-            fu = f(u);
-        }
-        ax = bx; bx = cx; cx = u;
-        fa = fb; fb = fc; fc = fu;
-    }
+    const double h = hi - lo;
+    const double d1 = slo + shi - 3.0 * (fhi - flo) / h;
+    const double disc = d1 * d1 - slo * shi;
+    if (!(disc >= 0.0)) return NAN;
+    const double d2 = std::copysign(std::sqrt(disc), h);
+    const double den = shi - slo + 2.0 * d2;
+    if (den == 0.0) return NAN;
+    return hi - h * (shi + d2 - d1) / den;
 }
 
-// Minimum of f bracketed by (ax, bx, cx): Brent's method, parabolic steps
-// when acceptable, golden-section steps otherwise.
-template <class F>
-double brent(F& f, double ax, double bx, double cx, double& xmin, double tol = 1.0e-8, int itmax = 10000)
+struct LinePoint {
+    double t, f, s;
+};
+
+// Minimum of phi(t) = f(p + t d) over t > 0 for a descent direction (slope
+// s0 < 0 at t = 0), from values and slopes (phi(t, &slope) returns the value).
+// Steps grow fourfold from t0 until the slope turns non-negative or the value
+// rises above the last descending point's, which brackets a minimum; the
+// bracket then shrinks around the Hermite-cubic minimiser of its ends, held to
+// the middle 80% of the bracket (else its midpoint).  Stops when the slope has
+// fallen below rtol |s0| or the bracket below rtol (|t| + rtol).  Returns the
+// lowest point evaluated.  The same search as dmft.py's line_minimum.
+template <class Phi>
+LinePoint line_minimum(Phi& phi, double f0, double s0, double t0, double rtol = 1.0e-10, int maxeval = 200)
 {
-    double a = std::min(ax, cx), b = std::max(ax, cx);
-    double x = bx, w = bx, v = bx;
-    double fx = f(x), fw = fx, fv = fx;
-    double d = 0.0, e = 0.0;
-    for (int it = 0; it < itmax; it++) {
-        const double xm = 0.5 * (a + b), tol1 = tol * std::fabs(x) + kZeps, tol2 = 2.0 * tol1;
-        if (std::fabs(x - xm) <= tol2 - 0.5 * (b - a)) { xmin = x; return fx; }
-        bool golden = true;
-        if (std::fabs(e) > tol1) {
-            double r = (x - w) * (fx - fv), q = (x - v) * (fx - fw), p = (x - v) * q - (x - w) * r;
-            q = 2.0 * (q - r);
-            if (q > 0.0) p = -p;
-            q = std::fabs(q);
-            const double etemp = e;
-            e = d;
-            if (!(std::fabs(p) >= std::fabs(0.5 * q * etemp) || p <= q * (a - x) || p >= q * (b - x))) {
-                d = p / q;
-                const double u = x + d;
-                if (u - a < tol2 || b - u < tol2) d = std::copysign(tol1, xm - x);
-                golden = false;
-            }
+    LinePoint lo{0.0, f0, s0}, hi{0.0, 0.0, 0.0}, best = lo;
+    bool have_hi = false;
+    double t = t0;
+    int n = 0;
+    while (!have_hi) {
+        double st = 0.0;
+        const double ft = phi(t, &st);
+        n++;
+        if (!std::isfinite(ft) || !std::isfinite(st)) {
+            hi = {t, INFINITY, INFINITY};
+            have_hi = true;
+            break;
         }
-        if (golden) {
-            e = (x >= xm) ? a - x : b - x;
-            d = kCGold * e;
+        if (ft < best.f) best = {t, ft, st};
+        if (st >= 0.0 || ft > lo.f) {
+            hi = {t, ft, st};
+            have_hi = true;
+            break;
         }
-        const double u = (std::fabs(d) >= tol1) ? x + d : x + std::copysign(tol1, d);
-        const double fu = f(u);
-        if (fu <= fx) {
-            if (u >= x) a = x; else b = x;
-            v = w; fv = fw; w = x; fw = fx; x = u; fx = fu;
-        } else {
-            if (u < x) a = u; else b = u;
-            if (fu <= fw || w == x) { v = w; fv = fw; w = u; fw = fu; }
-            else if (fu <= fv || v == x || v == w) { v = u; fv = fu; }
-        }
+        lo = {t, ft, st};
+        if (std::fabs(st) <= rtol * std::fabs(s0)) return best;
+        if (n >= maxeval) throw Fail{EDZT_ERR_NUMERIC, "bath fit: line search found no bracket"};
+        t *= 4.0;
     }
-    throw Fail{EDZT_ERR_NUMERIC, "bath fit: line minimisation did not converge"};
+    while (n < maxeval) {
+        const double w = hi.t - lo.t;
+        if (w <= rtol * (std::fabs(lo.t) + rtol)) break;
+        t = std::isfinite(hi.f) ? cubic_step(lo.t, lo.f, lo.s, hi.t, hi.f, hi.s) : NAN;
+        if (!(t >= lo.t + 0.1 * w && t <= hi.t - 0.1 * w)) t = lo.t + 0.5 * w;
+        double st = 0.0;
+        const double ft = phi(t, &st);
+        n++;
+        if (ft < best.f) best = {t, ft, st};
+        if (st < 0.0 && ft <= lo.f) lo = {t, ft, st};
+        else hi = {t, ft, st};
+        if (std::fabs(st) <= rtol * std::fabs(s0) && ft <= best.f) break;
+    }
+    return best;
 }
 
-// Polak-Ribiere conjugate gradient with exact line searches; stops when a
-// line search lowers f by less than ftol relative (ed_projection.f90 frprmn).
+double dot(const std::vector<double>& a, const std::vector<double>& b)
+{
+    double s = 0.0;
+    for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
+    return s;
+}
+
+// Nonlinear conjugate gradient with Polak-Ribiere directions (the reference's
+// fit method), restarted along the steepest descent when the update
+// coefficient is negative or the direction does not descend, with
+// line_minimum as the line search.  Stops when an iteration lowers f by no
+// more than ftol relative to f, 2 (f_old - f_new) <= ftol (|f_old| + |f_new|
+// + 1e-10 |f_start|), or when the gradient vanishes.  The same iteration as
+// dmft.py's conjugate_gradient.
 double conjugate_gradient(const BathFit& bf, std::vector<double>& p, double ftol, int* iters, int itmax = 20000)
 {
     const size_t n = p.size();
     double fp = bf.f(p);
-    std::vector<double> xi = bf.df(p), g(n), h(n);
-    for (size_t i = 0; i < n; i++) { g[i] = -xi[i]; h[i] = g[i]; xi[i] = h[i]; }
-    std::vector<double> pt(n);
+    const double floor = 1.0e-10 * std::fabs(fp);
+    std::vector<double> g = bf.df(p), d(n), q(n);
+    for (size_t i = 0; i < n; i++) d[i] = -g[i];
+    double step = 1.0;
     for (int it = 1; it <= itmax; it++) {
-        auto f1 = [&](double t) {
-            for (size_t i = 0; i < n; i++) pt[i] = p[i] + t * xi[i];
-            return bf.f(pt);
-        };
-        double ax = 0.0, bx = 1.0, cx = 0.0, t = 0.0;
-        bracket(f1, ax, bx, cx);
-        const double fret = brent(f1, ax, bx, cx, t);
-        for (size_t i = 0; i < n; i++) p[i] += t * xi[i];
-        if (2.0 * std::fabs(fret - fp) <= ftol * (std::fabs(fret) + std::fabs(fp) + 1.0e-10)) {
-            *iters = it;
-            return fret;
+        double s0 = dot(g, d);
+        if (!(s0 < 0.0)) {                               // not a descent direction: restart
+            for (size_t i = 0; i < n; i++) d[i] = -g[i];
+            s0 = dot(g, d);
+            if (!(s0 < 0.0)) { *iters = it; return fp; }
         }
-        fp = fret;
-        xi = bf.df(p);
-        double gg = 0.0, dgg = 0.0;
-        for (size_t i = 0; i < n; i++) { gg += g[i] * g[i]; dgg += (xi[i] + g[i]) * xi[i]; }
-        if (gg == 0.0) { *iters = it; return fret; }
-        const double gam = dgg / gg;
-        for (size_t i = 0; i < n; i++) { g[i] = -xi[i]; h[i] = g[i] + gam * h[i]; xi[i] = h[i]; }
+        auto phi = [&](double t, double* slope) {
+            for (size_t i = 0; i < n; i++) q[i] = p[i] + t * d[i];
+            *slope = dot(bf.df(q), d);
+            return bf.f(q);
+        };
+        const LinePoint lp = line_minimum(phi, fp, s0, step);
+        for (size_t i = 0; i < n; i++) p[i] += lp.t * d[i];
+        const std::vector<double> gn = bf.df(p);
+        const double fn = lp.f;
+        if (2.0 * (fp - fn) <= ftol * (std::fabs(fp) + std::fabs(fn) + floor)) {
+            *iters = it;
+            return fn;
+        }
+        double num = 0.0;
+        for (size_t i = 0; i < n; i++) num += gn[i] * (gn[i] - g[i]);
+        const double beta = std::max(0.0, num / dot(g, g));
+        for (size_t i = 0; i < n; i++) d[i] = -gn[i] + beta * d[i];
+        step = lp.t > 0.0 ? lp.t : 1.0;
+        g = gn;
+        fp = fn;
     }
     throw Fail{EDZT_ERR_NUMERIC, "bath fit: conjugate gradient did not converge"};
 }

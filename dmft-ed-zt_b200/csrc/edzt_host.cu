@@ -24,7 +24,6 @@
 
 namespace {
 
-std::atomic<long long> g_launches{0};
 
 struct EdztError {
     int code;
@@ -139,7 +138,11 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
-bool is_device_ptr(const void* p)
+// True for memory the kernels of a context on `device` read directly: device
+// memory of that GPU or managed memory.  Device memory of another GPU is an
+// argument error (a kernel would fault on it without peer access); host
+// memory, pinned or not, is staged through a copy.
+bool is_device_ptr(const void* p, int device)
 {
     if (!p) return false;
     cudaPointerAttributes at;
@@ -147,6 +150,9 @@ bool is_device_ptr(const void* p)
         cudaGetLastError();
         return false;
     }
+    if (at.type == cudaMemoryTypeDevice && at.device != device)
+        throw EdztError{EDZT_ERR_ARG, "vector argument is device memory of GPU " + std::to_string(at.device) +
+                                          ", not of the context's GPU " + std::to_string(device)};
     return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
@@ -203,7 +209,7 @@ struct edzt_ctx {
     double* pinned = nullptr;
     std::unique_ptr<DevBuf> scal;          // device scalars
     std::unique_ptr<DevBuf> dot_part;      // dot partials
-    long long launches_at_create = 0;
+    std::atomic<long long> launches{0};    // kernel launches issued by this context
     // fault-test settings (edzt_set_fault_test): pass cap, barrier wait limit, stalled CTA
     int dbg_pass_cap = 0;
     unsigned long long dbg_wait_ns = 0;
@@ -225,7 +231,7 @@ StrTable& str_table_ns(edzt_ctx* c, int ns, int n)
     t->str = std::make_unique<DevBuf>(sizeof(uint32_t) * (size_t)std::max(t->count, 1));
     t->rank = std::make_unique<DevBuf>(sizeof(int32_t) * ((size_t)1 << ns));
     launch_build_strings(ns, n, t->str->as<uint32_t>(), t->rank->as<int32_t>(), c->stream);
-    g_launches += 2;
+    c->launches += 2;
     CKLAUNCH();
     StrTable& ref = *t;
     c->str_tables.emplace(key, std::move(t));
@@ -257,7 +263,7 @@ OpsTable& ops_table_mt(edzt_ctx* c, ModelTables& mt, int n, int sigma)
                           t->e1->as<double>(), t->hcnt->as<uint8_t>(), t->hpk->as<uint32_t>(),
                           t->amp->as<double>(), t->imp->as<uint8_t>(), t->sub ? t->sub->as<int32_t>() : nullptr,
                           c->stream);
-    g_launches += 1;
+    c->launches += 1;
     CKLAUNCH();
     OpsTable& ref = *t;
     mt.ops.emplace(key, std::move(t));
@@ -418,7 +424,7 @@ struct InVec {
     Lease<double> tmp;
     InVec(edzt_ctx* c, const double* p, long long n)
     {
-        if (is_device_ptr(p)) { d = p; return; }
+        if (is_device_ptr(p, c->device)) { d = p; return; }
         tmp = Lease<double>(c->pool, (size_t)std::max(n, 1LL));
         if (n > 0) CK(cudaMemcpyAsync(tmp.p, p, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
         d = tmp.p;
@@ -433,7 +439,7 @@ struct OutVec {
     edzt_ctx* c;
     OutVec(edzt_ctx* cc, double* p, long long nn) : n(nn), c(cc)
     {
-        if (is_device_ptr(p)) { d = p; return; }
+        if (is_device_ptr(p, c->device)) { d = p; return; }
         host = p;
         tmp = Lease<double>(c->pool, (size_t)std::max(n, 1LL));
         d = tmp.p;
@@ -590,7 +596,7 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     CK(cudaEventRecord(c->ev0, c->stream));
     CK(launch_lanczos_persistent(B, d_jobs, d_st, d_pre, d_part, d_sw, c->status->as<int>(), c->stream));
     CK(cudaEventRecord(c->ev1, c->stream));
-    g_launches += 1;
+    c->launches += 1;
     int status = 0;
     CK(cudaMemcpyAsync(st.data(), d_st, bytes_st, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(&status, c->status->p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -626,7 +632,7 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
 double plain_dot(edzt_ctx* c, const double* x, const double* y, long long n)
 {
     launch_dot(x, y, n, c->dot_part->as<double>(), c->scal->as<double>(), c->stream);
-    g_launches += 2;
+    c->launches += 2;
     CK(cudaMemcpyAsync(c->pinned, c->scal->p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return c->pinned[0];
@@ -646,36 +652,36 @@ int plain_lanczos(edzt_ctx* c, const DevSector& S, const double* v_init, int max
     CK(cudaMemcpyAsync(w.p, v_init, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
     launch_swap_scale(v.p, w.p, n, nullptr, norm_v, c->stream);                // w = v_init / norm_v :130
     std::swap(v.p, w.p);
-    g_launches += 1;
+    c->launches += 1;
     if (eig) {                                                                 // :254-255
         CK(cudaMemsetAsync(eig, 0, sizeof(double) * n, c->stream));
         launch_axpy(eig, w.p, n, nullptr, coeff[0], 1.0, c->stream);
-        g_launches += 1;
+        c->launches += 1;
     }
     launch_hx(S, w.p, v.p, 0, c->stream);                                      // :132
-    g_launches += 1;
+    c->launches += 1;
     CKLAUNCH();
     int nstep;
     if (!coeff) a[0] = plain_dot(c, w.p, v.p, n);                              // :134
     if (maxnstep == 1) return 1;                                               // :137-141
     launch_axpy(v.p, w.p, n, nullptr, a[0], -1.0, c->stream);                  // :143
-    g_launches += 1;
+    c->launches += 1;
     if (!coeff) b[1] = std::sqrt(plain_dot(c, v.p, v.p, n));                   // :144
     int k = 2;
     for (;;) {
         if (b[k - 1] < 1.0e-16) { nstep = k - 1; if (!coeff) b[k - 1] = 0.0; break; }
         launch_swap_scale(w.p, v.p, n, nullptr, b[k - 1], c->stream);          // :152-156
-        g_launches += 1;
+        c->launches += 1;
         if (eig) {                                                             // :279
             launch_axpy(eig, w.p, n, nullptr, coeff[k - 1], 1.0, c->stream);
-            g_launches += 1;
+            c->launches += 1;
         }
         launch_hx(S, w.p, v.p, 1, c->stream);                                  // :158
-        g_launches += 1;
+        c->launches += 1;
         if (!coeff) a[k - 1] = plain_dot(c, w.p, v.p, n);                      // :159
         if (k >= maxnstep) { nstep = k; break; }                               // :161-164
         launch_axpy(v.p, w.p, n, nullptr, a[k - 1], -1.0, c->stream);          // :166
-        g_launches += 1;
+        c->launches += 1;
         if (!coeff) b[k] = std::sqrt(plain_dot(c, v.p, v.p, n));               // :167
         k = k + 1;
     }
@@ -705,7 +711,7 @@ double finish_eigvec(edzt_ctx* c, const DevSector& S, double* vec, double e0)
     Lease<double> v(c->pool, (size_t)n);
     launch_hx(S, vec, v.p, 0, c->stream);
     launch_axpy(v.p, vec, n, nullptr, e0, -1.0, c->stream);
-    g_launches += 6;
+    c->launches += 6;
     CKLAUNCH();
     return plain_dot(c, v.p, v.p, n);
 }
@@ -766,12 +772,12 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
             launch_rl_project_out(w, B, nv, hd, n, st);
             launch_rl_mdot(B, nv, w, n, part, hd + 8, st);
             launch_rl_project_out(w, B, nv, hd + 8, n, st);
-            g_launches += 6;
+            c->launches += 6;
         }
         RlVecs W{};
         W.p[0] = w;
         launch_rl_mdot(W, 1, w, n, part, hd + 16, st);
-        g_launches += 2;
+        c->launches += 2;
         CKLAUNCH();
         CK(cudaMemcpyAsync(hh, hd, sizeof(double) * 17, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -781,11 +787,11 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
     auto random_vector = [&](int nv, uint64_t stream_no) {
         for (int tries = 0; tries < 3; tries++) {
             launch_fill_start(V[nv], n, edzt_stream_key(key, stream_no + (uint64_t)tries), st);
-            g_launches += 1;
+            c->launches += 1;
             const double nrm2 = orth(V[nv], nv);
             if (nrm2 > 0.0) {
                 launch_rl_div(V[nv], V[nv], std::sqrt(nrm2), n, st);
-                g_launches += 1;
+                c->launches += 1;
                 return;
             }
         }
@@ -801,7 +807,7 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
             if (!V[j + 1]) V[j + 1] = take();
             double* w = V[j + 1];
             launch_hx(S, V[j], w, 0, st);
-            g_launches += 1;
+            c->launches += 1;
             R.nmult++;
             const double nrm2 = orth(w, j + 1);
             T[j][j] = hh[j] + hh[8 + j];
@@ -814,14 +820,14 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
                     T[j][j + 1] = T[j + 1][j] = 0.0;
                 } else {
                     launch_rl_div(w, w, beta, n, st);
-                    g_launches += 1;
+                    c->launches += 1;
                     T[j][j + 1] = T[j + 1][j] = beta;
                 }
             } else {
                 betam = invariant ? 0.0 : beta;
                 if (!invariant) {
                     launch_rl_div(w, w, beta, n, st);
-                    g_launches += 1;
+                    c->launches += 1;
                 }
             }
         }
@@ -850,7 +856,7 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
         for (int j = 0; j < m; j++) B.p[j] = V[j];
         for (int i = 0; i < kk; i++) O.p[i] = take();
         launch_rl_combine(O, kk, B, m, Yd, n, st);
-        g_launches += 1;
+        c->launches += 1;
         CKLAUNCH();
         CK(cudaStreamSynchronize(st));                   // Yk (pageable) consumed
         double* resid_vec = V[m];
@@ -879,17 +885,17 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
     O.p[0] = vec_out;
     for (int i = 1; i < nvec; i++) O.p[i] = take();
     launch_rl_combine(O, nvec, B, m, Yd, n, st);
-    g_launches += 1;
+    c->launches += 1;
     CKLAUNCH();
     for (int i = 0; i < nvec; i++) {
         const double nrm2 = orth(O.p[i], 0);             // |x_i|^2 only
         launch_rl_div(O.p[i], O.p[i], std::sqrt(nrm2), n, st);
-        g_launches += 1;
+        c->launches += 1;
         if (with_resid) {
             double* w = spare.back();
             launch_hx(S, O.p[i], w, 0, st);
             launch_axpy(w, O.p[i], n, nullptr, theta[i], -1.0, st);
-            g_launches += 2;
+            c->launches += 2;
             R.resid[i] = std::sqrt(std::max(orth(w, 0), 0.0));
         }
     }
@@ -1033,7 +1039,7 @@ void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnste
             if (sector_dim(c, nu, nd) <= 0) continue;
             DevSector S = make_sector(c, nu, nd);
             launch_fill_start(vin.p, S.dim, edzt_stream_key(seed, stream_of(i)), c->stream);   // :42-46
-            g_launches += 1;
+            c->launches += 1;
             SectorResult& r = res[i];
             r.a.assign(maxnstep, 0.0);
             r.b.assign(maxnstep, 0.0);
@@ -1166,7 +1172,7 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
                 ApplyCArgs A = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
                 launch_apply_c(A, g.gs, vin.p, c->stream);
             }
-            g_launches += 1;
+            c->launches += 1;
             std::vector<double> ha(maxnstep), hb(maxnstep);
             g.nstep = plain_lanczos(c, S, vin.p, maxnstep, ha.data(), hb.data(), &g.norm0, nullptr, nullptr);
             CK(cudaMemcpyAsync(g.a, ha.data(), sizeof(double) * maxnstep, cudaMemcpyHostToDevice, c->stream));
@@ -1195,7 +1201,7 @@ void green_runs(edzt_ctx* c, std::vector<GreenRun>& runs, int maxnstep, int nw, 
         Lease<CFJob> dj(c->pool, cj.size());
         CK(cudaMemcpyAsync(dj.p, cj.data(), sizeof(CFJob) * cj.size(), cudaMemcpyHostToDevice, c->stream));
         launch_cf(dj.p, (int)cj.size(), omega_dev, nw, c->stream, real_axis, eta);
-        g_launches += 1;
+        c->launches += 1;
         CKLAUNCH();
         CK(cudaStreamSynchronize(c->stream));
     }
@@ -1363,7 +1369,7 @@ void cluster_green_matrix_impl(edzt_ctx* c, int nspin, int maxnstep, int nw, con
                         launch_apply_c(applyc_args(c, c->gs_up, c->gs_dn, pm, b, ispin, g.nu, g.nd), c->gs_vec.p,
                                        tmp.p, c->stream);
                         launch_axpy(starts.back().p, tmp.p, n, nullptr, 1.0, 1.0, c->stream);
-                        g_launches += 3;
+                        c->launches += 3;
                         CK(cudaStreamSynchronize(c->stream));   // tmp goes back to the pool
                         g.start = starts.back().p;
                     }
@@ -1531,7 +1537,7 @@ void solve_wave(edzt_ctx* c, std::vector<BatchInst>& B, int i0, int i1, int maxn
         const long long n = sector_dim_ns(B[i].model.nsite, B[i].gs_up, B[i].gs_dn);
         launch_dot(B[i].gsvec.p, B[i].gsvec.p, n, c->dot_part->as<double>(), c->scal->as<double>(), c->stream);
         launch_scale_inv_sqrt(B[i].gsvec.p, n, c->scal->as<double>(), c->stream);
-        g_launches += 3;
+        c->launches += 3;
     }
     CKLAUNCH();
     // ---- Green's function runs of every instance (dmft_green.f90:47-126)
@@ -1794,7 +1800,7 @@ int server_step(edzt_server* sv)
         const long long n = sector_dim_ns(I.model.nsite, I.gs_up, I.gs_dn);
         launch_dot(I.gsvec.p, I.gsvec.p, n, c->dot_part->as<double>(), c->scal->as<double>(), c->stream);
         launch_scale_inv_sqrt(I.gsvec.p, n, c->scal->as<double>(), c->stream);
-        g_launches += 3;
+        c->launches += 3;
         const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
         q->runs = cluster_runs(I.model.norb, even, I.gs_up, I.gs_dn);
         for (GreenRun& g : q->runs) {
@@ -1839,7 +1845,7 @@ int server_step(edzt_server* sv)
             Lease<CFJob> dj(c->pool, cj.size());
             CK(cudaMemcpyAsync(dj.p, cj.data(), sizeof(CFJob) * cj.size(), cudaMemcpyHostToDevice, c->stream));
             launch_cf(dj.p, (int)cj.size(), sv->omega->as<double>(), nw, c->stream);
-            g_launches += 1;
+            c->launches += 1;
             CKLAUNCH();
         }
         std::vector<double> hg(std::max<size_t>(ng, 1) * 2 * nw);
@@ -1904,7 +1910,7 @@ cudaStream_t edzt_ctx_stream(const edzt_ctx* c) { return c->stream; }
 
 void edzt_ctx_set_error(edzt_ctx* c, const char* msg) { c->err = msg ? msg : ""; }
 
-void edzt_count_launches(long long n) { g_launches += n; }
+void edzt_count_launches(edzt_ctx* c, long long n) { c->launches += n; }
 
 int edzt_ctx_ready_sector(edzt_ctx* c, int nu, int nd, DevSector* S, const char** why)
 {
@@ -1950,7 +1956,6 @@ int edzt_ctx_create(int device, edzt_ctx** out)
         CK(cudaMallocHost((void**)&c->pinned, sizeof(double) * 32));
         CK(cudaEventCreate(&c->ev0));
         CK(cudaEventCreate(&c->ev1));
-        c->launches_at_create = g_launches.load();
     });
     if (rc != EDZT_OK) {
         edzt_ctx_destroy(c);
@@ -1976,7 +1981,7 @@ void edzt_ctx_destroy(edzt_ctx* c)
 
 const char* edzt_last_error(const edzt_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-long long edzt_launch_count(const edzt_ctx* c) { return c ? g_launches.load() - c->launches_at_create : 0; }
+long long edzt_launch_count(const edzt_ctx* c) { return c ? c->launches.load() : 0; }
 
 int edzt_get_stream(edzt_ctx* c, void** stream)
 {
@@ -2080,7 +2085,7 @@ int edzt_hx(edzt_ctx* c, int ne_up, int ne_dn, const double* x, double* y, int a
         OutVec yo(c, y, S.dim);
         if (accumulate) yo.preload();
         launch_hx(S, xi.d, yo.d, accumulate ? 1 : 0, c->stream);
-        g_launches += 1;
+        c->launches += 1;
         CKLAUNCH();
         yo.finish();
         CK(cudaStreamSynchronize(c->stream));
@@ -2102,7 +2107,7 @@ int edzt_apply_c(edzt_ctx* c, int ne_up, int ne_dn, const double* vec, int pm, i
         InVec vi(c, vec, sector_dim(c, ne_up, ne_dn));
         OutVec vo(c, vec_out, sector_dim(c, ou, od));
         launch_apply_c(A, vi.d, vo.d, c->stream);
-        g_launches += 1;
+        c->launches += 1;
         CKLAUNCH();
         vo.finish();
         CK(cudaStreamSynchronize(c->stream));
@@ -2251,7 +2256,7 @@ int edzt_gs_occupancy(edzt_ctx* c, int nspin, double* occ, double* docc)
         Lease<double> part(c->pool, (size_t)occ_partials_size());
         launch_gs_occ(c->gs_vec.p, su.str->as<uint32_t>(), sd.str->as<uint32_t>(), su.count, dim, norb, part.p,
                       c->stream);
-        g_launches += 1;
+        c->launches += 1;
         CKLAUNCH();
         std::vector<double> hp((size_t)occ_partials_size());
         CK(cudaMemcpyAsync(hp.data(), part.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, c->stream));

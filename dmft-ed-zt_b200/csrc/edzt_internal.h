@@ -159,7 +159,7 @@ struct edzt_ctx;
 int edzt_ctx_device(const edzt_ctx* c);
 cudaStream_t edzt_ctx_stream(const edzt_ctx* c);
 void edzt_ctx_set_error(edzt_ctx* c, const char* msg);
-void edzt_count_launches(long long n);
+void edzt_count_launches(edzt_ctx* c, long long n);
 // The sector of (nu, nd) when its tables already exist; else an error code
 // with the reason in *why.
 int edzt_ctx_ready_sector(edzt_ctx* c, int nu, int nd, DevSector* S, const char** why);

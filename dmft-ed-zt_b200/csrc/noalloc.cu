@@ -13,11 +13,15 @@
 // limits the sector to EDZT_NOALLOC_MAX_DIM states and the run to
 // EDZT_NOALLOC_MAX_STEPS steps.  The first call on each device looks the
 // array's address up (cudaGetSymbolAddress) with that device current; that
-// first call should come before any stream capture.  Calls share the one
-// array per device, so calls whose GPU work overlaps (two contexts or two host
-// threads on the same device) race and must be serialised by the caller.
+// first call should come before any stream capture.  The address is kept for
+// the life of the process, so cudaDeviceReset (which tears down the device's
+// context and with it the array) is not supported while the library is
+// loaded.  Calls share the one array per device, so calls whose GPU work
+// overlaps (two contexts or two host threads on the same device) race and
+// must be serialised by the caller.
 #include <cstring>
 #include <mutex>
+#include <stdexcept>
 #include <string>
 #include <cuda_runtime.h>
 #include "../../include/edzt.h"
@@ -72,20 +76,25 @@ int scratch_for(int device, unsigned char** out, std::string& why)
     return EDZT_OK;
 }
 
-bool is_device_ptr(const void* p)
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+// True when the kernel can read p directly: device memory of `device` or
+// managed memory.  Device memory of another GPU is rejected.
+bool is_device_ptr(const void* p, int device)
 {
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
+    if (at.type == cudaMemoryTypeDevice && at.device != device)
+        throw Fail{EDZT_ERR_ARG, "v_init is device memory of GPU " + std::to_string(at.device) +
+                                     ", not of the context's GPU " + std::to_string(device)};
     return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
-
-struct Fail {
-    int code;
-    std::string msg;
-};
 
 #define NA_CK(call)                                                                                \
     do {                                                                                           \
@@ -144,12 +153,16 @@ void run(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, 
     int G = lz_grid_size(device, smem, &block);
     if (G <= 0) throw Fail{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
     if (G > kMaxGrid) G = kMaxGrid;
+    if (J.ntiles < 4 * G) {                              // spread a small sector over the grid, as the allocating path does
+        J.rows = lz_rows_balanced(S.dn.count, J.rows, G);
+        J.ntiles = (S.dn.count + J.rows - 1) / J.rows;
+    }
     J.npart = J.ntiles < G ? J.ntiles : G;
     J.tile0 = 0;
     J.slot0 = 0;
     // The start vector is read in the first pass only, which writes YW[1];
     // a host vector is staged in YW[0], first overwritten by the second pass.
-    if (is_device_ptr(v_init)) {
+    if (is_device_ptr(v_init, device)) {
         J.src = v_init;
     } else {
         NA_CK(cudaMemcpyAsync(d_yw0, v_init, sizeof(double) * S.dim, cudaMemcpyHostToDevice, st));
@@ -159,12 +172,11 @@ void run(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, 
     std::memset(hs, 0, sizeof(hs));
     hs[0].active = 1;
     const long long hprefix[2] = {0, J.ntiles};
-    // what must start at zero: sync words (but the run counters), status, a, b
-    unsigned counters[64] = {};
-    counters[0] = 1u;                                    // runs going
-    counters[32] = 1u;                                   // their snapshot at the last barrier
+    // what must start at zero: the barrier's sync words (but the count of
+    // runs still going, one), status, a, b
+    const unsigned runs_going = 1u;
     NA_CK(cudaMemsetAsync(d_sync, 0, lz_sync_bytes(G), st));
-    NA_CK(cudaMemcpyAsync(d_sync + 64, counters, sizeof(counters), cudaMemcpyHostToDevice, st));
+    NA_CK(cudaMemcpyAsync(d_sync + 64, &runs_going, sizeof(unsigned), cudaMemcpyHostToDevice, st));
     NA_CK(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     NA_CK(cudaMemsetAsync(d_a, 0, sizeof(double) * 2 * EDZT_NOALLOC_MAX_STEPS, st));
     NA_CK(cudaMemcpyAsync(d_job, &J, sizeof(J), cudaMemcpyHostToDevice, st));
@@ -180,7 +192,7 @@ void run(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, 
     B.max_passes = 2 * maxnstep + 4;
     B.stall_cta = -1;
     NA_CK(launch_lanczos_persistent(B, d_job, d_state, d_prefix, d_part, d_sync, d_status, st));
-    edzt_count_launches(1);
+    edzt_count_launches(c, 1);
     int status = 0;
     NA_CK(cudaMemcpyAsync(hs, d_state, sizeof(hs), cudaMemcpyDeviceToHost, st));
     NA_CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -208,5 +220,8 @@ extern "C" int edzt_lanczos_iteration_noalloc(edzt_ctx* c, int ne_up, int ne_dn,
     } catch (const Fail& f) {
         edzt_ctx_set_error(c, f.msg.c_str());
         return f.code;
+    } catch (const std::exception& e) {
+        edzt_ctx_set_error(c, e.what());
+        return EDZT_ERR_CUDA;
     }
 }

@@ -16,12 +16,12 @@ src/dmft_lattice.f90:75-103), so that the CPU-runnable workload (nsite 6,
                  G_loc = int dos(x) / (em + D_cl + 1/G_cl - x) dx  (:128-170)
                  stop when sum |G_cl - G_loc|^2 / (norb nbath nw) < scf_tol
 
-The fit minimises the reference's cost with the reference's method: the
-Polak-Ribiere conjugate gradient with a line search by golden-ratio
-bracketing and Brent's parabolic minimisation (Press et al., Numerical
-Recipes, 2nd ed., sections 10.1, 10.2 and 10.6; R. Brent, Algorithms for
-Minimization without Derivatives, 1973), written here from those published
-algorithms with the reference's tolerances (ftol 1e-6, line tolerance 1e-8).
+The fit minimises the reference's cost (ed_projection.f90:154-250) by a
+nonlinear conjugate gradient with Polak-Ribiere directions, as the reference
+does, with a line search of this module's own design that uses the cost's
+analytic gradient (line_minimum: fourfold step growth to a bracket, then
+safeguarded Hermite-cubic steps).  ftol is the reference's relative stopping
+tolerance (1e-6 by default).
 The impurity solver is a callback: the GPU library (gpu_solver) or the CPU
 oracle (used by the tests) give the same loop.
 """
@@ -33,13 +33,6 @@ import os
 from dataclasses import dataclass, field
 
 import numpy as np
-
-GOLD = 1.618034
-CGOLD = 0.3819660
-GLIMIT = 100.0
-TINY = 1.0e-20
-ZEPS = 1.0e-10
-
 
 # ---------------------------------------------------------------------------
 # Green's functions on the Matsubara grid
@@ -133,124 +126,112 @@ class BathFit:
         return g
 
 
-def _bracket(f, ax, bx):
-    """Bracket a minimum of f starting from ax, bx: golden-ratio steps with
-    parabolic extrapolation limited to GLIMIT times the last step."""
-    fa, fb = f(ax), f(bx)
-    if fb > fa:
-        ax, bx, fa, fb = bx, ax, fb, fa
-    cx = bx + GOLD * (bx - ax)
-    fc = f(cx)
-    while fb > fc:
-        r = (bx - ax) * (fb - fc)
-        q = (bx - cx) * (fb - fa)
-        den = 2.0 * math.copysign(max(abs(q - r), TINY), q - r)
-        u = bx - ((bx - cx) * q - (bx - ax) * r) / den
-        ulim = bx + GLIMIT * (cx - bx)
-        if (bx - u) * (u - cx) > 0.0:                 # parabolic point between b and c
-            fu = f(u)
-            if fu < fc:
-                return bx, u, cx
-            if fu > fb:
-                return ax, bx, u
-            u = cx + GOLD * (cx - bx)
-            fu = f(u)
-        elif (cx - u) * (u - ulim) > 0.0:             # between c and its limit
-            fu = f(u)
-            if fu < fc:
-                bx, cx, u = cx, u, u + GOLD * (u - cx)
-                fb, fc, fu = fc, fu, f(u)
-        elif (u - ulim) * (ulim - cx) >= 0.0:         # limited to its maximum
-            u = ulim
-            fu = f(u)
-        else:                                         # rejected: golden step
-            u = cx + GOLD * (cx - bx)
-            fu = f(u)
-        ax, bx, cx = bx, cx, u
-        fa, fb, fc = fb, fc, fu
-    return ax, bx, cx
+def _cubic_step(lo, flo, slo, hi, fhi, shi):
+    """Minimiser of the cubic that matches value and slope at both ends of
+    [lo, hi] (Hermite interpolation); None when that cubic has no interior
+    minimum."""
+    h = hi - lo
+    d1 = slo + shi - 3.0 * (fhi - flo) / h
+    disc = d1 * d1 - slo * shi
+    if not disc >= 0.0:
+        return None
+    d2 = math.copysign(math.sqrt(disc), h)
+    den = shi - slo + 2.0 * d2
+    if den == 0.0:
+        return None
+    t = hi - h * (shi + d2 - d1) / den
+    return t if math.isfinite(t) else None
 
 
-def _brent(f, ax, bx, cx, tol=1.0e-8, itmax=10000):
-    """Minimum of f bracketed by (ax, bx, cx): Brent's method, parabolic steps
-    when they are acceptable and golden-section steps otherwise."""
-    a, b = min(ax, cx), max(ax, cx)
-    x = w = v = bx
-    fx = fw = fv = f(x)
-    d = e = 0.0
-    for _ in range(itmax):
-        xm = 0.5 * (a + b)
-        tol1 = tol * abs(x) + ZEPS
-        tol2 = 2.0 * tol1
-        if abs(x - xm) <= tol2 - 0.5 * (b - a):
-            return x, fx
-        golden = True
-        if abs(e) > tol1:
-            r = (x - w) * (fx - fv)
-            q = (x - v) * (fx - fw)
-            p = (x - v) * q - (x - w) * r
-            q = 2.0 * (q - r)
-            if q > 0.0:
-                p = -p
-            q = abs(q)
-            etemp = e
-            e = d
-            if not (abs(p) >= abs(0.5 * q * etemp) or p <= q * (a - x) or p >= q * (b - x)):
-                d = p / q
-                u = x + d
-                if u - a < tol2 or b - u < tol2:
-                    d = math.copysign(tol1, xm - x)
-                golden = False
-        if golden:
-            e = (a - x) if x >= xm else (b - x)
-            d = CGOLD * e
-        u = x + d if abs(d) >= tol1 else x + math.copysign(tol1, d)
-        fu = f(u)
-        if fu <= fx:
-            if u >= x:
-                a = x
-            else:
-                b = x
-            v, fv, w, fw, x, fx = w, fw, x, fx, u, fu
+def line_minimum(phi, f0, s0, t0, rtol=1.0e-10, maxeval=200):
+    """Minimum of phi(t) = f(p + t d) over t > 0 for a descent direction
+    (slope s0 < 0 at t = 0), from values and slopes: phi(t) -> (f, slope).
+
+    Search: steps grow fourfold from t0 until the slope turns non-negative or
+    the value rises above that of the last descending point `lo`, which
+    brackets a minimum between `lo` and that point `hi`.  The bracket then shrinks
+    around the Hermite-cubic minimiser of its two ends, held to the middle 80%
+    of the bracket (else its midpoint), keeping a descending point as `lo`.
+    Stops when the slope has fallen below rtol |s0| or the bracket below
+    rtol (|t| + rtol).  Returns (t, f, slope) of the lowest point evaluated."""
+    lo, flo, slo = 0.0, f0, s0
+    best = (0.0, f0, s0)
+    t = t0
+    hi = None
+    n = 0
+    while hi is None:
+        ft, st = phi(t)
+        n += 1
+        if not (math.isfinite(ft) and math.isfinite(st)):
+            hi, fhi, shi = t, math.inf, math.inf
+            break
+        if ft < best[1]:
+            best = (t, ft, st)
+        if st >= 0.0 or ft > flo:
+            hi, fhi, shi = t, ft, st
+            break
+        lo, flo, slo = t, ft, st
+        if abs(st) <= rtol * abs(s0):
+            return best
+        if n >= maxeval:
+            raise RuntimeError("line search found no bracket")
+        t = 4.0 * t
+    while n < maxeval:
+        w = hi - lo
+        if w <= rtol * (abs(lo) + rtol):
+            break
+        t = _cubic_step(lo, flo, slo, hi, fhi, shi) if math.isfinite(fhi) else None
+        if t is None or not (lo + 0.1 * w <= t <= hi - 0.1 * w):
+            t = lo + 0.5 * w
+        ft, st = phi(t)
+        n += 1
+        if ft < best[1]:
+            best = (t, ft, st)
+        if st < 0.0 and ft <= flo:
+            lo, flo, slo = t, ft, st
         else:
-            if u < x:
-                a = u
-            else:
-                b = u
-            if fu <= fw or w == x:
-                v, fv, w, fw = w, fw, u, fu
-            elif fu <= fv or v == x or v == w:
-                v, fv = u, fu
-    raise RuntimeError("line minimisation did not converge")
+            hi, fhi, shi = t, ft, st
+        if abs(st) <= rtol * abs(s0) and ft <= best[1]:
+            break
+    return best
 
 
-def conjugate_gradient(f, df, p, ftol=1.0e-6, itmax=20000, eps=1.0e-10):
-    """Polak-Ribiere conjugate gradient with exact line searches; stops when
-    a line search lowers f by less than ftol relative (ed_projection.f90
-    frprmn with tol 1e-6).  Returns (p, iterations, f(p))."""
+def conjugate_gradient(f, df, p, ftol=1.0e-6, itmax=20000):
+    """Nonlinear conjugate gradient with Polak-Ribiere directions, restarted
+    along the steepest descent whenever the update coefficient is negative or
+    the direction does not descend, and line minimisation by line_minimum.
+    Stops when an iteration lowers f by no more than ftol relative to f,
+    2 (f_old - f_new) <= ftol (|f_old| + |f_new| + 1e-10 |f_start|), where
+    the last term keeps a cost that falls towards zero from needing ever
+    smaller steps, or when the gradient vanishes.  Returns (p, iterations,
+    f(p))."""
     p = np.array(p, dtype=float)
-    fp = f(p)
-    xi = df(p)
-    g = -xi
-    h = g.copy()
-    xi = h.copy()
+    fp = float(f(p))
+    floor = 1.0e-10 * abs(fp)
+    g = np.asarray(df(p), dtype=float)
+    d = -g
+    step = 1.0
     for it in range(1, itmax + 1):
-        f1 = lambda t: f(p + t * xi)
-        ax, bx, cx = _bracket(f1, 0.0, 1.0)
-        t, fret = _brent(f1, ax, bx, cx)
-        p = p + t * xi
-        if 2.0 * abs(fret - fp) <= ftol * (abs(fret) + abs(fp) + eps):
-            return p, it, fret
-        fp = fret
-        xi = df(p)
-        gg = float(g @ g)
-        dgg = float((xi + g) @ xi)
-        if gg == 0.0:
-            return p, it, fret
-        gam = dgg / gg
-        g = -xi
-        h = g + gam * h
-        xi = h.copy()
+        s0 = float(g @ d)
+        if not s0 < 0.0:                           # not a descent direction: restart
+            d = -g
+            s0 = float(g @ d)
+            if not s0 < 0.0:
+                return p, it, fp
+
+        def phi(t):
+            q = p + t * d
+            return float(f(q)), float(np.asarray(df(q), dtype=float) @ d)
+
+        t, fn, _ = line_minimum(phi, fp, s0, step)
+        p = p + t * d
+        gn = np.asarray(df(p), dtype=float)
+        if 2.0 * (fp - fn) <= ftol * (abs(fp) + abs(fn) + floor):
+            return p, it, fn
+        beta = max(0.0, float(gn @ (gn - g)) / float(g @ g))
+        d = -gn + beta * d
+        step = t if t > 0.0 else 1.0
+        g, fp = gn, fn
     raise RuntimeError("conjugate gradient did not converge")
 
 

@@ -115,8 +115,11 @@ int edzt_lanczos_iteration(edzt_ctx *ctx, int ne_up, int ne_dn, const double *v_
  * any earlier allocating call on that sector after edzt_set_model, e.g.
  * edzt_hx or edzt_lanczos_iteration), else EDZT_ERR_STATE.  The first call
  * on each device looks the scratch array up with that device current and
- * should come before any stream capture.  The array is shared by all
- * contexts of a device: calls whose GPU work overlaps race. */
+ * should come before any stream capture; the address is kept until exit,
+ * so cudaDeviceReset is not supported while the library is loaded.  The
+ * array is shared by all contexts of a device: calls whose GPU work
+ * overlaps race.  v_init may be host memory, or device memory of the
+ * context's GPU (device memory of another GPU: EDZT_ERR_ARG). */
 #define EDZT_NOALLOC_MAX_DIM 262144
 #define EDZT_NOALLOC_MAX_STEPS 2048
 int edzt_lanczos_iteration_noalloc(edzt_ctx *ctx, int ne_up, int ne_dn, const double *v_init, int maxnstep,

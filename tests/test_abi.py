@@ -74,3 +74,56 @@ def test_struct_layouts_match_python_mirror(pkg, tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for field, _ in py._fields_:
             assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
+
+
+def _c_prototypes():
+    """{name: [parameter declarations]} of every function in include/edzt.h."""
+    src = open(os.path.join(ROOT, "include", "edzt.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(edzt_[a-z_0-9]+)\s*\(([^;{]*?)\)\s*;", src, flags=re.S):
+        params = [p.strip() for p in m.group(2).split(",") if p.strip() and p.strip() != "void"]
+        protos[m.group(1)] = params
+    return protos
+
+
+def _fortran_bindings():
+    """{C name: (dummy arguments, names passed by value)} from fortran/edzt_iface.f90."""
+    src = open(os.path.join(ROOT, "fortran", "edzt_iface.f90")).read()
+    src = re.sub(r"!.*", "", src)
+    src = re.sub(r"&\s*\n\s*", " ", src)                       # join continuation lines
+    out = {}
+    for m in re.finditer(r"(?:function|subroutine)\s+\w+\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)(.*?)end\s+(?:function|subroutine)",
+                         src, flags=re.S | re.I):
+        args = [a.strip().lower() for a in m.group(1).split(",") if a.strip()]
+        byval, cptr = set(), set()
+        for decl in re.findall(r"^\s*[^\n]*::[^\n]*$", m.group(3), flags=re.M):
+            attrs, names = decl.split("::", 1)
+            names = {n.strip().split("(")[0].lower() for n in names.split(",")}
+            if "value" in attrs.lower():
+                byval |= names
+            if "c_ptr" in attrs.lower():
+                cptr |= names
+        out[m.group(2)] = (args, byval, cptr)
+    return out
+
+
+def test_fortran_interface_matches_header(pkg):
+    """Every bind(C) interface of fortran/edzt_iface.f90 names an exported
+    entry point and has the C prototype's parameter count; a parameter the C
+    prototype takes by value (no pointer) is a Fortran value argument, and a
+    pointer parameter is passed by reference or as a type(c_ptr) value."""
+    protos = _c_prototypes()
+    binds = _fortran_bindings()
+    assert len(binds) >= 18
+    for name, (args, byval, cptr) in binds.items():
+        if name == "strlen":
+            continue
+        assert name in pkg.EXPORTS, name
+        params = protos[name]
+        assert len(args) == len(params), (name, args, params)
+        for a, p in zip(args, params):
+            if "*" in p:
+                assert a not in byval or a in cptr, (name, a, p)
+            else:
+                assert a in byval and a not in cptr, (name, a, p)
