@@ -10,15 +10,21 @@
  * (yw-choi/DMFT-ED-ZT) for the hot path, line by line where the reference is
  * explicit.  Every function cites the reference file:line it follows.
  *
- * Parity status: UNPINNED against the reference itself.  The reference ships
- * no tests, golden vectors or fixtures, and it cannot be built in this image
- * (no Fortran compiler, MPI, MKL or ARPACK; its module graph is also cyclic:
- * dmft_green -> lanczos_solver -> impurity_hamiltonian -> ed_projection ->
- * dmft_green).  The restatement is instead checked against independent
- * known-answer tests (dense diagonalisation, the U=0 free-fermion limit, the
- * atomic limit, sum rules, particle-hole and spin symmetry, Hermiticity) and
- * against a second, literal pure-Python transliteration of the reference
- * (oracle/ref_literal.py) on small sectors.
+ * Parity status: PINNED to the reference's own source.  The reference ships
+ * no tests, golden vectors or fixtures, and it cannot be compiled in this
+ * image (no Fortran compiler, MPI, MKL or ARPACK; its module graph is also
+ * cyclic: dmft_green -> lanczos_solver -> impurity_hamiltonian ->
+ * ed_projection -> dmft_green).  oracle/f90run.py instead translates the
+ * reference's hot-path procedures statement by statement and runs them;
+ * tests/golden/make_ref_golden.py records their outputs (with the SHA-256 of
+ * every reference file read) in tests/golden/ref_golden.npz, and
+ * tests/test_ref_golden.py holds this oracle to them: basis strings, hx (both
+ * py forms, one to three orbitals, spin-flip and pair hopping) and apply_c
+ * bit for bit, Lanczos coefficients, the ground state and G(i w) within 1e-12.
+ * It is further checked against independent known-answer tests (dense
+ * diagonalisation, the U=0 free-fermion limit, the atomic limit, sum rules,
+ * particle-hole and spin symmetry, Hermiticity) and a literal pure-Python
+ * transliteration (oracle/ref_literal.py).
  *
  * Deliberate, documented deviations from the reference (all also made by the
  * product so that both agree):
@@ -45,6 +51,11 @@
  *   - dstevx (MKL, src/lanczos_solver.f90:197) is replaced by Sturm-sequence
  *     bisection for the lowest eigenvalue plus inverse iteration for its
  *     eigenvector; only the lowest pair is ever used (src/lanczos_solver.f90:67-68).
+ *   - green_diag builds z = cmplx(gs%val, omega(iw)) without a kind argument
+ *     (src/dmft_green.f90:223,253), which Fortran evaluates in single
+ *     precision; here z keeps E0 and w in double precision, as the product
+ *     does.  Run literally, the reference's G(i w) differs from the double-
+ *     precision one by about 1e-7 (tests/test_ref_golden.py records it).
  *
  * Layout conventions follow the reference's Fortran column-major arrays:
  *   em(norb,2)        -> em[iorb + norb*ispin]

@@ -2,8 +2,9 @@
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
 bench.py's CPU legs as the checker; the product never imports it.
-Parity status: unpinned against the reference (no runnable reference, no
-reference tests); see the header of edzt_oracle.c for what pins it instead.
+Parity status: pinned to the reference's own source through the golden
+vectors of tests/golden/ref_golden.npz, which oracle/f90run.py computes by
+running the reference's Fortran procedures; see the header of edzt_oracle.c.
 """
 
 from __future__ import annotations
