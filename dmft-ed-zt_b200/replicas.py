@@ -52,9 +52,42 @@ def max_over_ranks(value: float, dist=None, device=None) -> float:
 
 
 def gather_to_root(obj, dist=None, world: int = 1):
-    """Every rank's picklable result on rank 0 (list by rank); [obj] alone."""
+    """Every rank's picklable result, on every rank (list by rank); [obj] alone."""
     if dist is None or world == 1:
         return [obj]
     out = [None] * world
     dist.all_gather_object(out, obj)
     return out
+
+
+def instance_cost(inst, maxnstep: int) -> float:
+    """Cost of one impurity solve for the partition: the sum over its Lanczos
+    runs of dimension x steps (ground-state scan and eigenvector pass of every
+    sector, plus the c / c^+ runs of the ground-state sector's neighbours,
+    bounded by the largest neighbouring dimension)."""
+    from math import comb
+    m = inst["model"]
+    ns = m.nsite
+    dims = [comb(ns, u) * comb(ns, d) for u, d in inst["sectors"]]
+    nruns = 4 * m.norb if int(inst.get("nspin", 1)) == 2 else 2 * m.norb
+    return float(maxnstep) * (2.0 * sum(dims) + nruns * max(dims))
+
+
+def sharded_batch(solve_batch, instances, maxnstep: int, rank: int, world: int, dist=None):
+    """The batched form over `world` ranks: rank `rank` solves its LPT share
+    of the instances (by instance_cost) with solve_batch(list) -> dict of
+    isector [n], e0 [n] and G_cl (list of n arrays); the shares are gathered
+    to every rank and returned in instance order, with this rank's indices.
+    No data-path collective: the only exchange is the final gather of the
+    small results."""
+    costs = [instance_cost(inst, maxnstep) for inst in instances]
+    mine = my_units(costs, rank, world)
+    part = solve_batch([instances[i] for i in mine]) if mine else {"isector": [], "e0": [], "G_cl": []}
+    local = (mine, [int(v) for v in part["isector"]], [float(v) for v in part["e0"]], list(part["G_cl"]))
+    shares = gather_to_root(local, dist, world)
+    n = len(instances)
+    isector, e0, G = [None] * n, [None] * n, [None] * n
+    for idx, isec, ee, gg in shares:
+        for j, i in enumerate(idx):
+            isector[i], e0[i], G[i] = isec[j], ee[j], gg[j]
+    return {"isector": isector, "e0": e0, "G_cl": G}, mine

@@ -156,7 +156,10 @@ def test_green_diag_matches_cluster(solver, bethe):
 
 
 def test_solve_aim_n12(solver, configs, oracle_mod):
-    """The large single-solve workload (nsite 12, 9 sectors, 300 steps) end to end."""
+    """The large single-solve workload (nsite 12, 9 sectors, 300 steps) end
+    to end: E0, G(i w_n) on 2048 points, and the first 50 continued-fraction
+    coefficients a_n, b_n of the c^+ and the c run (src/dmft_green.f90:204-250;
+    excitation sectors of 731,808 states)."""
     cfg = configs.aim_n12()
     o = oracle_for(oracle_mod, cfg["model"])
     gs_ref = o.ground_state(cfg["sectors"], cfg["maxnstep"], seed=0)
@@ -167,6 +170,16 @@ def test_solve_aim_n12(solver, configs, oracle_mod):
     r = solver.solve(cfg["sectors"], cfg["maxnstep"], omega, nspin=1, seed=0)
     assert r["isector"] == gs_ref["isector"] and _e_ok(r["e0"], gs_ref["e0"])
     assert np.abs(r["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
+    gs = solver.ground_state(cfg["sectors"], cfg["maxnstep"], seed=0)
+    assert gs["isector"] == gs_ref["isector"]
+    cg = solver.cluster_green_ftn(1, cfg["maxnstep"], omega)
+    assert np.abs(cg["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
+    c, cr = cg["coeffs"], cg_ref["coeffs"]
+    for q in (0, 2):                       # (a^+, b^+) and (a^-, b^-) of the impurity orbital, spin up
+        k = ab_compare_len(cr[0, 0, q + 1], cfg["maxnstep"])
+        assert k == 50
+        assert np.abs(c[0, 0, q, :k] - cr[0, 0, q, :k]).max() <= AB_TOL
+        assert np.abs(c[0, 0, q + 1, :k] - cr[0, 0, q + 1, :k]).max() <= AB_TOL
 
 
 @pytest.mark.parametrize("nspin", [1, 2])
