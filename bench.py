@@ -27,10 +27,12 @@ and seeded: the reference quotes no data set.
              per GPU (on N GPUs each rank solves its cost-balanced share),
              solves/s, with the plain engine's solves/s on the same instances
              (one per nsite timed, weighted by counts)
-  served     the served form (one GPU): --served requests, Poisson arrivals at
-             200/s, nsite 8..12, through edzt_server's request loop: solves/s
-             and p50/p99 latency from arrival to result, with the plain
-             engine's solves/s on the same requests
+  served     the served form (one GPU): --served requests of the workload's
+             nsite 8..16 distribution, Poisson arrivals at 200/s (saturation),
+             through edzt_server's request loop: solves/s and p50/p99 latency
+             from arrival to result; a second run below saturation (half the
+             measured throughput) with the small requests' p50 against their
+             solve-alone time; the plain engine's solves/s on the same requests
 
 --impl reference times the CPU oracle on all host threads (the reference
 itself is Fortran + MPI + MKL and cannot be built here).
@@ -212,14 +214,9 @@ def batched_leg(pkg, s, cfgs, n, dist=None, rank=0, world=1):
     return out
 
 
-def served_leg(pkg, s, cfgs, n, seed=5, nsite_max=12):
-    """The served form: n requests with Poisson arrivals (mean 200 req/s),
-    nsite ~ U{8..nsite_max} (the workload's distribution is U{8..16}; the
-    default run stops at 12 to stay within minutes), random U, J = 0, bath as
-    the batched form, nspin 2, through edzt_server's request loop."""
+def _served_requests(pkg, cfgs, n, seed, nsite_max):
     import numpy as np
     rng = np.random.default_rng(seed)
-    omega = pkg.matsubara(2048, 100.0)
     reqs = []
     for _ in range(n):
         ns = int(rng.integers(8, nsite_max + 1))
@@ -230,26 +227,76 @@ def served_leg(pkg, s, cfgs, n, seed=5, nsite_max=12):
         m = pkg.Model(1, nb, np.zeros((1, 2)), np.stack([ek, ek], 1), np.stack([V, V], 1).reshape(1, nb, 2),
                       U=U, mu=U / 2)
         reqs.append(dict(model=m, sectors=cfgs.near_half_sectors(ns), nspin=2, seed=int(rng.integers(1 << 40))))
-    arrivals = np.cumsum(rng.exponential(1.0 / 200.0, n))
-    arrivals -= arrivals[0]
+    return reqs, rng
+
+
+def _serve_run(pkg, s, reqs, arrivals, omega):
     sv = pkg.Server(s, 300, omega)
     try:
-        sv.submit(reqs[0])
-        for _ in range(4):                                   # warm-up
-            sv.step()
         _, lat, total = pkg.serve(sv, reqs, arrivals)
     finally:
         sv.close()
+    return lat, total
+
+
+def served_leg(pkg, s, cfgs, n, seed=5, nsite_max=16, sub=12):
+    """The served form, requests of the workload's distribution: nsite ~
+    U{8..nsite_max}, random U, J = 0, bath as the batched form, nspin 2,
+    through edzt_server's request loop (pkg.serve), latency from arrival to
+    result.
+      saturation    n requests, Poisson arrivals at 200/s (seed 5): solves/s,
+                    p50/p99 overall and by nsite
+      sub-saturation  `sub` requests of a second draw (seed 6), Poisson at
+                    half the measured saturation throughput: p50/p99, and the
+                    p50 of the small requests (nsite <= 11) against their
+                    solve-alone time (edzt_solve on the same request)
+    with the plain engine's solves/s on the saturation requests (one request
+    per nsite timed, weighted by counts)."""
+    import numpy as np
+    import torch
+    omega = pkg.matsubara(2048, 100.0)
+    reqs, rng = _served_requests(pkg, cfgs, n, seed, nsite_max)
+    arrivals = np.cumsum(rng.exponential(1.0 / 200.0, n))
+    arrivals -= arrivals[0]
+    warm = _served_requests(pkg, cfgs, 2, 99, 10)[0]                 # warm-up: tables, pool, kernels
+    _serve_run(pkg, s, warm, [0.0, 0.0], omega)
+    lat, total = _serve_run(pkg, s, reqs, arrivals, omega)
+    ns = np.array([r["model"].nsite for r in reqs])
+    by_ns = {int(k): round(float(np.percentile(lat[ns == k], 50)) * 1000, 1) for k in sorted(set(ns.tolist()))}
+    rate_sat = n / total
+    # below saturation
+    sreqs, srng = _served_requests(pkg, cfgs, sub, seed + 1, nsite_max)
+    offered = 0.5 * rate_sat
+    sarr = np.cumsum(srng.exponential(1.0 / offered, sub))
+    sarr -= sarr[0]
+    slat, stotal = _serve_run(pkg, s, sreqs, sarr, omega)
+    sns = np.array([r["model"].nsite for r in sreqs])
+    small = np.nonzero(sns <= 11)[0]
+    alone = []
+    for i in small:
+        r = sreqs[i]
+        s.set_model(r["model"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.solve(r["sectors"], 300, omega, nspin=2, seed=r["seed"])
+        torch.cuda.synchronize()
+        alone.append(time.perf_counter() - t0)
+    sub_out = {"requests": sub, "offered_rate_per_s": offered, "seconds": stotal,
+               "latency_ms": {"p50": float(np.percentile(slat, 50) * 1000), "p99": float(np.percentile(slat, 99) * 1000)}}
+    if small.size:
+        sub_out["small_requests"] = {
+            "count": int(small.size), "p50_ms": float(np.percentile(slat[small], 50) * 1000),
+            "alone_p50_ms": float(np.percentile(alone, 50) * 1000),
+            "ratio": float(np.percentile(slat[small], 50) / np.percentile(alone, 50)),
+            "how": "nsite <= 11; alone = edzt_solve of the same request on the idle GPU, host wall clock"}
     plain, per_ns = plain_estimate(pkg, s, reqs, omega, 300)
-    return {"value": n / total, "unit": "solves/s", "requests": n, "seconds": total,
+    return {"value": rate_sat, "unit": "solves/s", "requests": n, "seconds": total,
             "latency_ms": {"p50": float(np.percentile(lat, 50) * 1000), "p99": float(np.percentile(lat, 99) * 1000)},
-            "offered_rate_per_s": 200.0,
+            "p50_ms_by_nsite": by_ns, "offered_rate_per_s": 200.0, "sub_saturation": sub_out,
             "plain_gpu": {"value": plain, "unit": "solves/s", "ms_per_solve_by_nsite": per_ns,
                           "how": "one request per nsite timed, weighted by counts"},
-            "sample": (f"{n} requests, nsite 8..{nsite_max}" +
-                       (" of the 8..16 distribution (nsite 13..16 solves take seconds each and do not fit the "
-                        "default run's time bound; --served-nsite-max 16 runs all)" if nsite_max < 16 else "") +
-                       ", Poisson 200/s (seed 5)")}
+            "sample": f"{n} requests, nsite ~ U{{8..{nsite_max}}}, Poisson 200/s (seed 5); the sub-saturation "
+                      f"run: {sub} requests (seed 6) at half the measured throughput"}
 
 
 def hv_leg(pkg, s, peak):
@@ -598,7 +645,7 @@ def run_gpu(args):
         batched = batched_leg(pkg, s, cfgs, args.batched, dist, rank, world)
     if world == 1 and args.served > 0:
         cfgs = importlib.import_module("dmft_ed_zt_b200.configs")
-        served = served_leg(pkg, s, cfgs, args.served, nsite_max=args.served_nsite_max)
+        served = served_leg(pkg, s, cfgs, args.served, nsite_max=args.served_nsite_max, sub=args.served_sub)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -693,8 +740,9 @@ def main():
     ap.add_argument("--skip-hv", action="store_true")
     ap.add_argument("--batched", type=int, default=256, help="instances of the batched leg (0: skip)")
     ap.add_argument("--served", type=int, default=32, help="requests of the served leg (0: skip)")
-    ap.add_argument("--served-nsite-max", type=int, default=12, choices=range(8, 17),
-                    help="largest nsite of the served leg's requests (the workload's is 16)")
+    ap.add_argument("--served-nsite-max", type=int, default=16, choices=range(8, 17),
+                    help="largest nsite of the served leg's requests (the workload's 16 by default)")
+    ap.add_argument("--served-sub", type=int, default=12, help="requests of the served leg's sub-saturation run")
     ap.add_argument("--traffic-file", default=os.path.join(ROOT, "profiles", "k_lanczos_aim_n12_dram.txt"))
     ap.add_argument("--case", default=None, help="run one small profiling case (hx:NS, lz:NS, solve) and exit")
     args = ap.parse_args()

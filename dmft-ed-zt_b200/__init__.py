@@ -51,7 +51,7 @@ EXPORTS = (
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
     "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
     "edzt_cluster_green_matrix", "edzt_gs_occupancy", "edzt_green_real", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
-    "edzt_server_cancel", "edzt_instance_footprint", "edzt_set_fault_test", "edzt_diag_arpack",
+    "edzt_server_cancel", "edzt_server_set_step_ms", "edzt_instance_footprint", "edzt_set_fault_test", "edzt_diag_arpack",
     "edzt_set_diag_solver", "edzt_hybridization", "edzt_local_green_bethe", "edzt_fit_bath", "edzt_dmft_bethe",
 )
 # ground_state's diag_solver values (src/ground_state.f90:53-60).
@@ -185,6 +185,7 @@ def load_library(path: str = LIB_PATH):
     L.edzt_server_destroy.argtypes = [_vp]
     L.edzt_server_destroy.restype = None
     L.edzt_server_cancel.argtypes = [_vp, C.c_longlong]
+    L.edzt_server_set_step_ms.argtypes = [_vp, C.c_double]
     L.edzt_instance_footprint.argtypes = [_vp, C.POINTER(C.c_longlong)]
     L.edzt_set_fault_test.argtypes = [_vp, C.c_int, C.c_double, C.c_int]
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
@@ -631,6 +632,10 @@ class Server:
 
     def cancel(self, rid: int):
         self.solver._check(self._L.edzt_server_cancel(self._h, rid))
+
+    def set_step_ms(self, ms: float):
+        """Time budget of one step (edzt_server_set_step_ms)."""
+        self.solver._check(self._L.edzt_server_set_step_ms(self._h, C.c_double(ms)))
 
     def close(self):
         if self._h:

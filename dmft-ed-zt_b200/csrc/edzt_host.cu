@@ -200,7 +200,6 @@ struct edzt_ctx {
     Lease<double> gs_vec;
     // persistent-kernel scratch
     std::unique_ptr<DevBuf> sync_words, status;
-    int grid_cache_smem = -1, grid_cache = 0, block_cache = 256;
     // persistent-kernel statistics
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long st_launches = 0;
@@ -307,6 +306,9 @@ DevSector make_sector_mt(edzt_ctx* c, ModelTables& mt, int nu, int nd)
     fill(S.dn, sd, od);
     S.dim = (long long)su.count * sd.count;
     arg_check(S.dim < (1LL << 32), "sector dimension must stay below 2^32 states");
+    arg_check(hx_fits(su.count, sd.count),
+              "sector too large for the shared-memory staging of H.v (more than 13,000 strings of a spin: "
+              "beyond nsite 16 at half filling)");
     S.P = mt.P;
     S.has_j = mt.has_j ? 1 : 0;
     S.wint = mt.wint->as<double>();
@@ -484,24 +486,15 @@ struct JobSpec {
     double norm0 = 0.0;
 };
 
-int persistent_grid(edzt_ctx* c, size_t smem, int* block)
-{
-    if ((int)smem != c->grid_cache_smem) {
-        c->grid_cache = lz_grid_size(c->device, smem, &c->block_cache);
-        c->grid_cache_smem = (int)smem;
-    }
-    *block = c->block_cache;
-    return c->grid_cache;
-}
-
 void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
 {
     const int nj = (int)specs.size();
     if (nj == 0) return;
     std::vector<LzJob> jobs(nj);
     std::vector<Lease<double2>> bufs;
+    std::vector<Lease<double>> dbufs;
     bufs.reserve((size_t)nj * 2);
-    size_t smem = 0;
+    dbufs.reserve((size_t)nj);
     int max_steps = 0;
     for (int j = 0; j < nj; j++) {
         JobSpec& s = specs[j];
@@ -513,6 +506,8 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
             bufs.emplace_back(c->pool, (size_t)dim);
             J.YW[q] = bufs.back().p;
         }
+        dbufs.emplace_back(c->pool, (size_t)dim);
+        J.D = dbufs.back().p;
         J.eig = s.eig;
         J.coeff = s.coeff;
         J.a = s.a;
@@ -523,60 +518,36 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
         J.key = s.key;
         J.ac = s.ac;
         J.src = s.ac_src;
-        J.rows = lz_rows_per_tile(J.S.up.count, J.S.dn.count, J.S.dn.hw);
-        J.ntiles = (J.S.dn.count + J.rows - 1) / J.rows;
-        smem = std::max(smem, lz_smem_bytes(J.S.up.count, J.S.dn.hw, J.rows));
         max_steps = std::max(max_steps, J.maxnstep);
         if (s.mode == LZ_COEFF) {
             CK(cudaMemsetAsync(s.a, 0, sizeof(double) * s.maxnstep, c->stream));
             CK(cudaMemsetAsync(s.b, 0, sizeof(double) * s.maxnstep, c->stream));
         }
     }
-    int block = 256;
-    const int G = persistent_grid(c, smem, &block);
-    if (G <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
-    // A launch with few tiles (one or a few sectors) spreads each job evenly
-    // over the grid with smaller tiles; a launch with many (a batch) keeps
-    // the largest tiles, since every tile costs a staging round and two CTA
-    // barriers whatever its size.
-    long long tiles_max = 0;
-    for (int j = 0; j < nj; j++) tiles_max += jobs[j].ntiles;
-    if (tiles_max < 4LL * G) {
-        for (int j = 0; j < nj; j++) {
-            LzJob& J = jobs[j];
-            J.rows = lz_rows_balanced(J.S.dn.count, J.rows, G);
-            J.ntiles = (J.S.dn.count + J.rows - 1) / J.rows;
-        }
-    }
-    // tiles of all jobs in one list; CTA b takes tiles b, b+G, ...; the
-    // participants of job j are CTAs (tile0 + q) mod G, q < min(G, ntiles)
-    std::vector<long long> prefix(nj + 1, 0);
-    long long slots = 0;
-    for (int j = 0; j < nj; j++) {
-        LzJob& J = jobs[j];
-        J.tile0 = prefix[j];
-        prefix[j + 1] = prefix[j] + J.ntiles;
-        J.npart = std::min(G, J.ntiles);
-        J.slot0 = slots;
-        slots += J.npart;
-    }
+    // rows per tile and columns per slab of every job, tile lists of both
+    // phases, grid and shared memory (lz_plan)
+    std::vector<long long> prefix;
+    const LzPlan P = lz_plan(c->device, jobs.data(), nj, prefix);
+    if (P.grid <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
+    const int G = P.grid;
     std::vector<LzState> st(2 * (size_t)nj);
     std::memset(st.data(), 0, sizeof(LzState) * st.size());
-    for (int j = 0; j < nj; j++) st[2 * (size_t)j].active = 1;
+    for (int j = 0; j < nj; j++) st[2 * (size_t)j + 1].active = 1;   // the state before phase 0 (parity 1)
     const size_t bytes_jobs = sizeof(LzJob) * nj, bytes_st = sizeof(LzState) * st.size();
-    const size_t bytes_pre = sizeof(long long) * (nj + 1), bytes_part = sizeof(double) * 8 * (size_t)slots;
+    const size_t bytes_pre = sizeof(long long) * prefix.size(), bytes_slots = sizeof(double) * 2 * (size_t)P.slots;
     const size_t bytes_sw = lz_sync_bytes(G);
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t total = al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part) + al(bytes_sw);
+    const size_t total = al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_slots) + al(bytes_sw);
     Lease<char> blob(c->pool, total);
     char* base = blob.p;
     LzJob* d_jobs = reinterpret_cast<LzJob*>(base);
     LzState* d_st = reinterpret_cast<LzState*>(base + al(bytes_jobs));
     long long* d_pre = reinterpret_cast<long long*>(base + al(bytes_jobs) + al(bytes_st));
-    double* d_part = reinterpret_cast<double*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre));
-    unsigned* d_sw = reinterpret_cast<unsigned*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_part));
+    double* d_slots = reinterpret_cast<double*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre));
+    unsigned* d_sw = reinterpret_cast<unsigned*>(base + al(bytes_jobs) + al(bytes_st) + al(bytes_pre) + al(bytes_slots));
     std::vector<unsigned> sw(bytes_sw / sizeof(unsigned), 0u);
     sw[64] = (unsigned)nj;   // runs still going
+    for (int j = 0; j < nj; j++) jobs[j].st = d_st + 2 * (size_t)j;
     CK(cudaMemcpyAsync(d_jobs, jobs.data(), bytes_jobs, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(d_st, st.data(), bytes_st, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(d_pre, prefix.data(), bytes_pre, cudaMemcpyHostToDevice, c->stream));
@@ -586,15 +557,16 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     std::memset(&B, 0, sizeof(B));
     B.njobs = nj;
     B.grid = G;
-    B.block = block;
-    B.smem = smem;
-    B.total_tiles = prefix[nj];
-    B.max_passes = 2 * max_steps + 4;   // start vector, every step, and room for repeated steps
-    if (c->dbg_pass_cap > 0) B.max_passes = std::min(B.max_passes, c->dbg_pass_cap);
+    B.block = P.block;
+    B.smem = P.smem;
+    B.total[0] = P.total[0];
+    B.total[1] = P.total[1];
+    B.max_phases = 2 * max_steps + 4;   // two phases per step and the phase that closes the last one
+    if (c->dbg_pass_cap > 0) B.max_phases = std::min(B.max_phases, c->dbg_pass_cap);
     B.wait_ns = c->dbg_wait_ns;
     B.stall_cta = c->dbg_stall_cta;
     CK(cudaEventRecord(c->ev0, c->stream));
-    CK(launch_lanczos_persistent(B, d_jobs, d_st, d_pre, d_part, d_sw, c->status->as<int>(), c->stream));
+    CK(launch_lanczos_persistent(B, d_jobs, d_pre, d_slots, d_sw, c->status->as<int>(), c->stream));
     CK(cudaEventRecord(c->ev1, c->stream));
     c->launches += 1;
     int status = 0;
@@ -643,7 +615,7 @@ int plain_lanczos(edzt_ctx* c, const DevSector& S, const double* v_init, int max
                   double* norm_out, const double* coeff, double* eig)
 {
     const long long n = S.dim;
-    Lease<double> v(c->pool, (size_t)n), w(c->pool, (size_t)n);
+    Lease<double> v(c->pool, (size_t)n), w(c->pool, (size_t)n), hs(c->pool, (size_t)n);
     if (coeff == nullptr)
         for (int i = 0; i < maxnstep; i++) { a[i] = 0.0; b[i] = 0.0; }
     const double norm_v = std::sqrt(plain_dot(c, v_init, v_init, n));          // :128
@@ -658,8 +630,8 @@ int plain_lanczos(edzt_ctx* c, const DevSector& S, const double* v_init, int max
         launch_axpy(eig, w.p, n, nullptr, coeff[0], 1.0, c->stream);
         c->launches += 1;
     }
-    launch_hx(S, w.p, v.p, 0, c->stream);                                      // :132
-    c->launches += 1;
+    launch_hx(S, w.p, v.p, 0, hs.p, c->stream);                                // :132
+    c->launches += 2;
     CKLAUNCH();
     int nstep;
     if (!coeff) a[0] = plain_dot(c, w.p, v.p, n);                              // :134
@@ -676,8 +648,8 @@ int plain_lanczos(edzt_ctx* c, const DevSector& S, const double* v_init, int max
             launch_axpy(eig, w.p, n, nullptr, coeff[k - 1], 1.0, c->stream);
             c->launches += 1;
         }
-        launch_hx(S, w.p, v.p, 1, c->stream);                                  // :158
-        c->launches += 1;
+        launch_hx(S, w.p, v.p, 1, hs.p, c->stream);                            // :158
+        c->launches += 2;
         if (!coeff) a[k - 1] = plain_dot(c, w.p, v.p, n);                      // :159
         if (k >= maxnstep) { nstep = k; break; }                               // :161-164
         launch_axpy(v.p, w.p, n, nullptr, a[k - 1], -1.0, c->stream);          // :166
@@ -708,10 +680,10 @@ double finish_eigvec(edzt_ctx* c, const DevSector& S, double* vec, double e0)
     double* sc = c->scal->as<double>();
     launch_dot(vec, vec, n, c->dot_part->as<double>(), sc, c->stream);
     launch_scale_inv_sqrt(vec, n, sc, c->stream);                              // :291
-    Lease<double> v(c->pool, (size_t)n);
-    launch_hx(S, vec, v.p, 0, c->stream);
+    Lease<double> v(c->pool, (size_t)n), hs(c->pool, (size_t)n);
+    launch_hx(S, vec, v.p, 0, hs.p, c->stream);
     launch_axpy(v.p, vec, n, nullptr, e0, -1.0, c->stream);
-    c->launches += 6;
+    c->launches += 7;
     CKLAUNCH();
     return plain_dot(c, v.p, v.p, n);
 }
@@ -752,7 +724,7 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
     const int m = kArNcv, kmax = kArNev + (kArNcv - kArNev) / 2;
     const double eps = 0x1p-53, eps23 = std::pow(eps, 2.0 / 3.0), tol = eps;
     cudaStream_t st = c->stream;
-    Lease<double> buf(c->pool, (size_t)(m + 1 + kmax) * n);
+    Lease<double> buf(c->pool, (size_t)(m + 1 + kmax) * n), hxs(c->pool, (size_t)n);
     Lease<double> small(c->pool, (size_t)rl_partials_size() + 32 + EDZT_RL_MAXV * EDZT_RL_MAXV);
     double* part = small.p;
     double* hd = small.p + rl_partials_size();          // [0, 8) pass 1, [8, 16) pass 2, [16] |w|^2
@@ -806,8 +778,8 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
         for (int j = k; j < m; j++) {                    // extend the factorisation to m vectors
             if (!V[j + 1]) V[j + 1] = take();
             double* w = V[j + 1];
-            launch_hx(S, V[j], w, 0, st);
-            c->launches += 1;
+            launch_hx(S, V[j], w, 0, hxs.p, st);
+            c->launches += 2;
             R.nmult++;
             const double nrm2 = orth(w, j + 1);
             T[j][j] = hh[j] + hh[8 + j];
@@ -893,9 +865,9 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
         c->launches += 1;
         if (with_resid) {
             double* w = spare.back();
-            launch_hx(S, O.p[i], w, 0, st);
+            launch_hx(S, O.p[i], w, 0, hxs.p, st);
             launch_axpy(w, O.p[i], n, nullptr, theta[i], -1.0, st);
-            c->launches += 2;
+            c->launches += 3;
             R.resid[i] = std::sqrt(std::max(orth(w, 0), 0.0));
         }
     }
@@ -1583,14 +1555,14 @@ void init_inst(const edzt_instance& in, BatchInst& I)
         const int nu = I.sec[2 * s], nd = I.sec[2 * s + 1];
         arg_check(sector_valid_ns(ns, nu, nd), "electron counts outside [0, nsite]");
         const long long d = sector_dim_ns(ns, nu, nd);
-        gsb += 32 * d;
+        gsb += 40 * d;                                   // two pair buffers and D per run
         maxd = std::max(maxd, d);
         for (int du = -1; du <= 1; du++)
             for (int dd = -1; dd <= 1; dd++)
                 if ((du == 0) != (dd == 0)) maxe = std::max(maxe, sector_dim_ns(ns, nu + du, nd + dd));
     }
-    const long long cfb = 4LL * I.model.norb * 32 * maxe + 8 * maxd;
-    I.footprint = std::max(gsb, cfb) + 48 * maxd;
+    const long long cfb = 4LL * I.model.norb * 40 * maxe + 8 * maxd;
+    I.footprint = std::max(gsb, cfb) + 56 * maxd;
 }
 
 void solve_batch_impl(edzt_ctx* c, int ninst, const edzt_instance* inst, int maxnstep, int nw, const double* omega,
@@ -1628,19 +1600,38 @@ void solve_batch_impl(edzt_ctx* c, int ninst, const edzt_instance* inst, int max
 }
 
 // ---------------------------------------------------------------------------
-// served form: continuous batching of impurity solves.  A request advances
-// one phase per step (sector scan, eigenvector pass, c / c^+ runs with the
-// continued fractions); every step is one persistent launch that carries the
-// current phase of every active request, and requests queued meanwhile are
-// admitted at the next step when their device-memory footprint fits.
+// served form: continuous batching of impurity solves at the granularity of
+// Lanczos phases.  A request goes through three phases (sector scan,
+// eigenvector pass, c / c^+ runs with the continued fractions); the Lanczos
+// runs of a phase are live jobs whose buffers and recurrence state persist
+// across launches.  Every step serves one size class of requests (classes
+// by nsite, the small ones together, taken in turn): it runs slices of that
+// class's live runs (persistent launches of a budget of phases, ending with
+// every unfinished run's next step opened, so a later launch resumes it)
+// and moves requests on as their phase's runs finish, until the step's time
+// budget is spent or the class has nothing left to run.  Requests queued
+// meanwhile are admitted at the next step when their device-memory
+// footprint fits; a small request is thus never held behind the scans of
+// large ones for longer than their steps' time budgets.
 // ---------------------------------------------------------------------------
+struct LiveJob {
+    JobSpec spec;
+    DevSector S{};
+    Lease<double2> yw0, yw1;
+    Lease<double> d;
+    Lease<LzState> st;                     // [2] by phase parity, on the device
+    int k = 0;                             // steps done (host view, from the last slice)
+    bool done = false;
+};
+
 struct ServReq {
     long long id = 0;
     BatchInst I;
     int phase = 0;                         // 1 scan, 2 eigenvector, 3 Green's runs, 4 done
+    int cls = 0;                           // size class
     bool cancelled = false;
     Lease<double> ab;                      // [nsector][2][maxnstep] scan coefficients (device)
-    std::vector<int> job_of_sector;        // scan job of each sector in the current launch, -1 if none
+    std::vector<int> job_of_sector;        // live scan job of each sector, -1 if none
     std::vector<double> hab;               // scan coefficients on the host
     std::vector<SectorResult> res;
     int win = -1;                          // winning sector
@@ -1648,6 +1639,7 @@ struct ServReq {
     std::vector<GreenRun> runs;
     Lease<double> gab;                     // [nruns][2][maxnstep] Green's-run coefficients (device)
     std::vector<double> G;                 // G_cl(nw, norb, nspin), complex interleaved
+    std::vector<std::unique_ptr<LiveJob>> jobs;   // the live runs of the current phase
     std::string error;
 };
 
@@ -1658,12 +1650,134 @@ struct edzt_server {
     int maxnstep = 0, nw = 0;
     std::unique_ptr<DevBuf> omega;
     long long budget = 0, reserved = 0, next_id = 1;
+    double step_ms = 25.0;                 // time budget of one step
+    int last_cls = -1;                     // class served by the last step
+    std::map<int, double> ms_per_phase;    // measured phase time by class
     std::deque<std::unique_ptr<ServReq>> queue;
     std::vector<std::unique_ptr<ServReq>> active;
     std::map<long long, std::unique_ptr<ServReq>> finished;
 };
 
 namespace {
+
+// Size class of a request: its nsite, the requests up to nsite 11 together.
+int size_class(const BatchInst& I) { return std::max(I.model.nsite, 11); }
+
+std::unique_ptr<LiveJob> make_live(edzt_ctx* c, const JobSpec& spec)
+{
+    auto L = std::make_unique<LiveJob>();
+    L->spec = spec;
+    L->S = make_sector_mt(c, spec.mt ? *spec.mt : c->mt, spec.nu, spec.nd);
+    L->yw0 = Lease<double2>(c->pool, (size_t)L->S.dim);
+    L->yw1 = Lease<double2>(c->pool, (size_t)L->S.dim);
+    L->d = Lease<double>(c->pool, (size_t)L->S.dim);
+    L->st = Lease<LzState>(c->pool, 2);
+    LzState init[2];
+    std::memset(init, 0, sizeof(init));
+    init[1].active = 1;                                  // the state before the first phase (parity 1)
+    CK(cudaMemcpyAsync(L->st.p, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));                // init (host memory) consumed
+    if (spec.mode == LZ_COEFF) {
+        CK(cudaMemsetAsync(spec.a, 0, sizeof(double) * spec.maxnstep, c->stream));
+        CK(cudaMemsetAsync(spec.b, 0, sizeof(double) * spec.maxnstep, c->stream));
+    }
+    return L;
+}
+
+// One slice: at most `phases` phases (even) of every live run in v, in one
+// persistent launch; runs that finish are marked done with nstep and norm0.
+// Returns the launch's device time in ms.
+float run_slice(edzt_ctx* c, std::vector<LiveJob*>& v, int phases)
+{
+    const int nj = (int)v.size();
+    std::vector<LzJob> jobs(nj);
+    for (int j = 0; j < nj; j++) {
+        LiveJob& L = *v[j];
+        LzJob& J = jobs[j];
+        std::memset(&J, 0, sizeof(J));
+        J.S = L.S;
+        J.YW[0] = L.yw0.p;
+        J.YW[1] = L.yw1.p;
+        J.D = L.d.p;
+        J.eig = L.spec.eig;
+        J.coeff = L.spec.coeff;
+        J.a = L.spec.a;
+        J.b = L.spec.b;
+        J.maxnstep = L.spec.maxnstep;
+        J.mode = L.spec.mode;
+        J.init = L.spec.init;
+        J.key = L.spec.key;
+        J.ac = L.spec.ac;
+        J.src = L.spec.ac_src;
+        J.st = L.st.p;
+    }
+    std::vector<long long> prefix;
+    const LzPlan P = lz_plan(c->device, jobs.data(), nj, prefix);
+    if (P.grid <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t bytes_jobs = sizeof(LzJob) * nj, bytes_pre = sizeof(long long) * prefix.size();
+    const size_t bytes_slots = sizeof(double) * 2 * (size_t)P.slots, bytes_sw = lz_sync_bytes(P.grid);
+    Lease<char> blob(c->pool, al(bytes_jobs) + al(bytes_pre) + al(bytes_slots) + al(bytes_sw));
+    LzJob* d_jobs = reinterpret_cast<LzJob*>(blob.p);
+    long long* d_pre = reinterpret_cast<long long*>(blob.p + al(bytes_jobs));
+    double* d_slots = reinterpret_cast<double*>(blob.p + al(bytes_jobs) + al(bytes_pre));
+    unsigned* d_sw = reinterpret_cast<unsigned*>(blob.p + al(bytes_jobs) + al(bytes_pre) + al(bytes_slots));
+    std::vector<unsigned> sw(bytes_sw / sizeof(unsigned), 0u);
+    sw[64] = (unsigned)nj;
+    CK(cudaMemcpyAsync(d_jobs, jobs.data(), bytes_jobs, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_pre, prefix.data(), bytes_pre, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_sw, sw.data(), bytes_sw, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->status->p, 0, sizeof(int), c->stream));
+    LzBatch B;
+    std::memset(&B, 0, sizeof(B));
+    B.njobs = nj;
+    B.grid = P.grid;
+    B.block = P.block;
+    B.smem = P.smem;
+    B.total[0] = P.total[0];
+    B.total[1] = P.total[1];
+    B.max_phases = std::max(2, phases & ~1);
+    if (c->dbg_pass_cap > 0) B.max_phases = std::min(B.max_phases, std::max(2, c->dbg_pass_cap & ~1));
+    B.wait_ns = c->dbg_wait_ns;
+    B.stall_cta = c->dbg_stall_cta;
+    B.slice = 1;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    CK(launch_lanczos_persistent(B, d_jobs, d_pre, d_slots, d_sw, c->status->as<int>(), c->stream));
+    CK(cudaEventRecord(c->ev1, c->stream));
+    c->launches += 1;
+    std::vector<LzState> st(2 * (size_t)nj);
+    for (int j = 0; j < nj; j++)
+        CK(cudaMemcpyAsync(&st[2 * (size_t)j], v[j]->st.p, 2 * sizeof(LzState), cudaMemcpyDeviceToHost, c->stream));
+    int status = 0;
+    CK(cudaMemcpyAsync(&status, c->status->p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (status == EDZT_DEV_BARRIER_TIMEOUT)
+        throw EdztError{EDZT_ERR_TIMEOUT, "persistent Lanczos kernel: grid barrier wait timed out"};
+    if (status != 0) throw EdztError{EDZT_ERR_CUDA, "persistent Lanczos kernel reported status " + std::to_string(status)};
+    double bytes = 0.0;
+    for (int j = 0; j < nj; j++) {
+        LiveJob& L = *v[j];
+        const LzState& s0 = st[2 * (size_t)j];
+        const LzState& s1 = st[2 * (size_t)j + 1];
+        const LzState* fin = !s0.active ? &s0 : (!s1.active ? &s1 : nullptr);
+        const int k_now = fin ? fin->nstep : std::max(s0.k, s1.k) - 1;   // an opened step is not done yet
+        const double per_step = (L.spec.mode == LZ_COEFF) ? 24.0 : 40.0;
+        if (L.k == 0 && k_now > 0) bytes += (double)L.S.dim * ((L.spec.init == LZ_INIT_HASH) ? 8.0 : 16.0);
+        bytes += (double)L.S.dim * per_step * std::max(0, k_now - L.k);
+        L.k = std::max(L.k, k_now);
+        if (fin) {
+            L.done = true;
+            L.spec.nstep = fin->nstep;
+            L.spec.norm0 = fin->norm0;
+        }
+    }
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->st_launches += 1;
+    c->st_ms += ms;
+    c->st_bytes += bytes;
+    return ms;
+}
 
 void server_admit(edzt_server* sv)
 {
@@ -1676,191 +1790,222 @@ void server_admit(edzt_server* sv)
         set_tables_model(*q.I.mt, q.I.model, c->stream);
         const int ns = (int)q.I.sec.size() / 2;
         q.ab = Lease<double>(c->pool, (size_t)std::max(ns, 1) * 2 * sv->maxnstep);
+        q.cls = size_class(q.I);
         q.phase = 1;
+        // the scan: one run per sector (ground_state.f90:28-73)
+        const int nsite = q.I.model.nsite;
+        q.job_of_sector.assign(ns, -1);
+        for (int s = 0; s < ns; s++) {
+            const int nu = q.I.sec[2 * s], nd = q.I.sec[2 * s + 1];
+            if (sector_dim_ns(nsite, nu, nd) <= 0) continue;
+            JobSpec j;
+            j.mt = q.I.mt.get();
+            j.nu = nu; j.nd = nd;
+            j.mode = LZ_COEFF;
+            j.init = LZ_INIT_HASH;
+            j.key = edzt_stream_key(q.I.seed, (uint64_t)s);
+            j.maxnstep = sv->maxnstep;
+            j.a = q.ab.p + (size_t)(2 * s) * sv->maxnstep;
+            j.b = q.ab.p + (size_t)(2 * s + 1) * sv->maxnstep;
+            q.job_of_sector[s] = (int)q.jobs.size();
+            q.jobs.push_back(make_live(c, j));
+        }
         sv->active.push_back(std::move(sv->queue.front()));
         sv->queue.pop_front();
     }
 }
 
-// One step: the current phase of every active request in one launch.
-int server_step(edzt_server* sv)
+bool phase_done(const ServReq& q)
+{
+    for (const auto& j : q.jobs)
+        if (!j->done) return false;
+    return true;
+}
+
+// Scan finished: the tridiagonal ground state of every sector, the winner
+// (ground_state.f90:62-68, 1e-10 tie band) and its eigenvector pass.
+void after_scan(edzt_server* sv, ServReq& q)
+{
+    edzt_ctx* c = sv->c;
+    const int maxnstep = sv->maxnstep;
+    const int nsec = (int)q.I.sec.size() / 2;
+    q.hab.assign((size_t)std::max(nsec, 1) * 2 * maxnstep, 0.0);
+    CK(cudaMemcpyAsync(q.hab.data(), q.ab.p, sizeof(double) * q.hab.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    q.res.assign(nsec, SectorResult{});
+    for (int s = 0; s < nsec; s++) {
+        const int jq = q.job_of_sector[s];
+        if (jq < 0) continue;
+        SectorResult& r = q.res[s];
+        r.nstep = q.jobs[jq]->spec.nstep;
+        if (r.nstep < 1) continue;
+        r.coeff.resize(r.nstep);
+        r.ok = edzt::lowest_eigenpair(r.nstep, q.hab.data() + (size_t)(2 * s) * maxnstep,
+                                      q.hab.data() + (size_t)(2 * s + 1) * maxnstep, &r.e, r.coeff.data()) == 0;
+    }
+    int w = -1;
+    for (int s = 0; s < nsec; s++) {
+        if (!q.res[s].ok) continue;
+        const double tie = 1.0e-10 * std::max(1.0, std::fabs(w < 0 ? 0.0 : q.res[w].e));
+        if (w < 0 || q.res[s].e < q.res[w].e - tie) w = s;
+    }
+    q.jobs.clear();
+    if (w < 0) { q.error = "no sector produced a ground state"; q.phase = 4; return; }
+    q.win = w;
+    q.I.best = w;
+    q.I.gs_up = q.I.sec[2 * w]; q.I.gs_dn = q.I.sec[2 * w + 1];
+    q.I.e0 = q.res[w].e;
+    q.I.gsvec = Lease<double>(c->pool, (size_t)sector_dim_ns(q.I.model.nsite, q.I.gs_up, q.I.gs_dn));
+    q.coef = Lease<double>(c->pool, (size_t)q.res[w].nstep);
+    CK(cudaMemcpyAsync(q.coef.p, q.res[w].coeff.data(), sizeof(double) * q.res[w].nstep, cudaMemcpyHostToDevice,
+                       c->stream));
+    JobSpec j;                                            // eigenvector pass (lanczos_solver.f90:213-300)
+    j.mt = q.I.mt.get();
+    j.nu = q.I.gs_up; j.nd = q.I.gs_dn;
+    j.mode = LZ_EIGVEC;
+    j.init = LZ_INIT_HASH;
+    j.key = edzt_stream_key(q.I.seed, (uint64_t)w);
+    j.maxnstep = q.res[w].nstep;
+    j.coeff = q.coef.p;
+    j.eig = q.I.gsvec.p;
+    j.a = q.ab.p + (size_t)(2 * w) * maxnstep;
+    j.b = q.ab.p + (size_t)(2 * w + 1) * maxnstep;
+    q.jobs.push_back(make_live(c, j));
+    q.phase = 2;
+}
+
+// Eigenvector pass finished: normalise it (lanczos_solver.f90:291) and start
+// the c / c^+ runs (dmft_green.f90:204-250).
+void after_eigvec(edzt_server* sv, ServReq& q)
+{
+    edzt_ctx* c = sv->c;
+    const int maxnstep = sv->maxnstep;
+    BatchInst& I = q.I;
+    const long long n = sector_dim_ns(I.model.nsite, I.gs_up, I.gs_dn);
+    launch_dot(I.gsvec.p, I.gsvec.p, n, c->dot_part->as<double>(), c->scal->as<double>(), c->stream);
+    launch_scale_inv_sqrt(I.gsvec.p, n, c->scal->as<double>(), c->stream);
+    c->launches += 3;
+    CKLAUNCH();
+    const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
+    q.runs = cluster_runs(I.model.norb, even, I.gs_up, I.gs_dn);
+    q.gab = Lease<double>(c->pool, std::max<size_t>(q.runs.size(), 1) * 2 * maxnstep);
+    CK(cudaMemsetAsync(q.gab.p, 0, sizeof(double) * std::max<size_t>(q.runs.size(), 1) * 2 * maxnstep, c->stream));
+    q.jobs.clear();
+    const int ns = I.model.nsite;
+    for (size_t r = 0; r < q.runs.size(); r++) {
+        GreenRun& g = q.runs[r];
+        g.mt = I.mt.get();
+        g.gs = I.gsvec.p;
+        g.gs_up = I.gs_up; g.gs_dn = I.gs_dn;
+        g.e0 = I.e0;
+        g.a = q.gab.p + (2 * r) * maxnstep;
+        g.b = q.gab.p + (2 * r + 1) * maxnstep;
+        g.nstep = 0;
+        if (sector_dim_ns(ns, g.nu, g.nd) <= 0) continue;
+        JobSpec j;
+        j.mt = I.mt.get();
+        j.nu = g.nu; j.nd = g.nd;
+        j.mode = LZ_COEFF;
+        j.init = LZ_INIT_APPLYC;
+        j.ac = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
+        j.ac_src = g.gs;
+        j.maxnstep = maxnstep;
+        j.a = g.a; j.b = g.b;
+        g.nstep = -1 - (int)q.jobs.size();              // its live run, resolved when it finishes
+        q.jobs.push_back(make_live(c, j));
+    }
+    q.phase = 3;
+}
+
+// Green's runs finished: continued fractions and G_cl.
+void after_green(edzt_server* sv, ServReq& q)
 {
     edzt_ctx* c = sv->c;
     const int maxnstep = sv->maxnstep, nw = sv->nw;
-    server_admit(sv);
-    std::vector<JobSpec> specs;
-    for (auto& up : sv->active)                               // cancelled requests leave now
-        if (up->cancelled) { up->error = "cancelled"; up->phase = 4; }
-    for (auto& up : sv->active) {
-        ServReq& q = *up;
-        BatchInst& I = q.I;
-        const int ns = I.model.nsite;
-        if (q.phase == 1) {                                   // sector scan (ground_state.f90:28-73)
-            const int nsec = (int)I.sec.size() / 2;
-            q.job_of_sector.assign(nsec, -1);
-            for (int s = 0; s < nsec; s++) {
-                const int nu = I.sec[2 * s], nd = I.sec[2 * s + 1];
-                if (sector_dim_ns(ns, nu, nd) <= 0) continue;
-                JobSpec j;
-                j.mt = I.mt.get();
-                j.nu = nu; j.nd = nd;
-                j.mode = LZ_COEFF;
-                j.init = LZ_INIT_HASH;
-                j.key = edzt_stream_key(I.seed, (uint64_t)s);
-                j.maxnstep = maxnstep;
-                j.a = q.ab.p + (size_t)(2 * s) * maxnstep;
-                j.b = q.ab.p + (size_t)(2 * s + 1) * maxnstep;
-                q.job_of_sector[s] = (int)specs.size();
-                specs.push_back(j);
-            }
-        } else if (q.phase == 2) {                            // eigenvector pass (lanczos_solver.f90:213-300)
-            const SectorResult& r = q.res[q.win];
-            JobSpec j;
-            j.mt = I.mt.get();
-            j.nu = I.gs_up; j.nd = I.gs_dn;
-            j.mode = LZ_EIGVEC;
-            j.init = LZ_INIT_HASH;
-            j.key = edzt_stream_key(I.seed, (uint64_t)q.win);
-            j.maxnstep = r.nstep;
-            j.coeff = q.coef.p;
-            j.eig = I.gsvec.p;
-            j.a = q.ab.p + (size_t)(2 * q.win) * maxnstep;
-            j.b = q.ab.p + (size_t)(2 * q.win + 1) * maxnstep;
-            specs.push_back(j);
-        } else if (q.phase == 3) {                            // c / c^+ runs (dmft_green.f90:204-250)
-            for (size_t r = 0; r < q.runs.size(); r++) {
-                GreenRun& g = q.runs[r];
-                g.a = q.gab.p + (2 * r) * maxnstep;
-                g.b = q.gab.p + (2 * r + 1) * maxnstep;
-                g.nstep = 0;
-                if (sector_dim_ns(ns, g.nu, g.nd) <= 0) continue;
-                JobSpec j;
-                j.mt = I.mt.get();
-                j.nu = g.nu; j.nd = g.nd;
-                j.mode = LZ_COEFF;
-                j.init = LZ_INIT_APPLYC;
-                j.ac = applyc_args_ns(c, ns, g.gs_up, g.gs_dn, g.pm, g.iorb, g.ispin, g.nu, g.nd);
-                j.ac_src = g.gs;
-                j.maxnstep = maxnstep;
-                j.a = g.a; j.b = g.b;
-                g.nstep = -1 - (int)specs.size();             // its job, resolved after the launch
-                specs.push_back(j);
-            }
+    BatchInst& I = q.I;
+    std::vector<CFJob> cj;
+    const size_t ng = q.runs.size();
+    Lease<double> g(c->pool, std::max<size_t>(ng, 1) * 2 * nw);
+    CK(cudaMemsetAsync(g.p, 0, sizeof(double) * std::max<size_t>(ng, 1) * 2 * nw, c->stream));
+    for (size_t r = 0; r < ng; r++) {
+        GreenRun& gr = q.runs[r];
+        if (gr.nstep < 0) {
+            const LiveJob& L = *q.jobs[-1 - gr.nstep];
+            gr.nstep = L.spec.nstep;
+            gr.norm0 = L.spec.norm0;
         }
+        if (gr.nstep < 1) continue;
+        CFJob J;
+        J.a = gr.a; J.b = gr.b;
+        J.b1 = gr.norm0;
+        J.levels = (gr.nstep == 1 && maxnstep >= 2) ? 2 : gr.nstep;
+        J.zr_shift = (gr.pm == 1) ? gr.e0 : -gr.e0;
+        J.sign = (gr.pm == 1) ? -1.0 : 1.0;
+        J.g = g.p + r * 2 * nw;
+        cj.push_back(J);
     }
-    if (!specs.empty()) run_jobs(c, specs);
-
-    // after the launch: every request moves one phase on
-    std::vector<ServReq*> scan, eig, green;
-    for (auto& up : sv->active) {
-        if (up->phase == 1) scan.push_back(up.get());
-        else if (up->phase == 2) eig.push_back(up.get());
-        else if (up->phase == 3) green.push_back(up.get());
+    if (!cj.empty()) {
+        Lease<CFJob> dj(c->pool, cj.size());
+        CK(cudaMemcpyAsync(dj.p, cj.data(), sizeof(CFJob) * cj.size(), cudaMemcpyHostToDevice, c->stream));
+        launch_cf(dj.p, (int)cj.size(), sv->omega->as<double>(), nw, c->stream);
+        c->launches += 1;
+        CKLAUNCH();
+        CK(cudaStreamSynchronize(c->stream));              // dj and its CF jobs consumed
     }
-    for (ServReq* q : scan) {                                 // tridiagonal ground state per sector
-        const int nsec = (int)q->I.sec.size() / 2;
-        q->hab.assign((size_t)std::max(nsec, 1) * 2 * maxnstep, 0.0);
-        CK(cudaMemcpyAsync(q->hab.data(), q->ab.p, sizeof(double) * q->hab.size(), cudaMemcpyDeviceToHost,
-                           c->stream));
-    }
+    std::vector<double> hg(std::max<size_t>(ng, 1) * 2 * nw);
+    CK(cudaMemcpyAsync(hg.data(), g.p, sizeof(double) * hg.size(), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    for (ServReq* q : scan) {
-        const int nsec = (int)q->I.sec.size() / 2;
-        q->res.assign(nsec, SectorResult{});
-        parallel_for(nsec, [&](int s) {
-            const int jq = q->job_of_sector[s];
-            if (jq < 0) return;
-            SectorResult& r = q->res[s];
-            r.nstep = specs[jq].nstep;
-            if (r.nstep < 1) return;
-            r.coeff.resize(r.nstep);
-            r.ok = edzt::lowest_eigenpair(r.nstep, q->hab.data() + (size_t)(2 * s) * maxnstep,
-                                          q->hab.data() + (size_t)(2 * s + 1) * maxnstep, &r.e,
-                                          r.coeff.data()) == 0;
-        });
-        int w = -1;                                           // ground_state.f90:62-68, 1e-10 tie band
-        for (int s = 0; s < nsec; s++) {
-            if (!q->res[s].ok) continue;
-            const double tie = 1.0e-10 * std::max(1.0, std::fabs(w < 0 ? 0.0 : q->res[w].e));
-            if (w < 0 || q->res[s].e < q->res[w].e - tie) w = s;
-        }
-        if (w < 0) { q->error = "no sector produced a ground state"; q->phase = 4; continue; }
-        q->win = w;
-        q->I.best = w;
-        q->I.gs_up = q->I.sec[2 * w]; q->I.gs_dn = q->I.sec[2 * w + 1];
-        q->I.e0 = q->res[w].e;
-        q->I.gsvec = Lease<double>(c->pool, (size_t)sector_dim_ns(q->I.model.nsite, q->I.gs_up, q->I.gs_dn));
-        q->coef = Lease<double>(c->pool, (size_t)q->res[w].nstep);
-        CK(cudaMemcpyAsync(q->coef.p, q->res[w].coeff.data(), sizeof(double) * q->res[w].nstep,
-                           cudaMemcpyHostToDevice, c->stream));
-        q->phase = 2;
-    }
-    for (ServReq* q : eig) {                                  // normalise (lanczos_solver.f90:291), plan the runs
-        BatchInst& I = q->I;
-        const long long n = sector_dim_ns(I.model.nsite, I.gs_up, I.gs_dn);
-        launch_dot(I.gsvec.p, I.gsvec.p, n, c->dot_part->as<double>(), c->scal->as<double>(), c->stream);
-        launch_scale_inv_sqrt(I.gsvec.p, n, c->scal->as<double>(), c->stream);
-        c->launches += 3;
-        const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
-        q->runs = cluster_runs(I.model.norb, even, I.gs_up, I.gs_dn);
-        for (GreenRun& g : q->runs) {
-            g.mt = I.mt.get();
-            g.gs = I.gsvec.p;
-            g.gs_up = I.gs_up; g.gs_dn = I.gs_dn;
-            g.e0 = I.e0;
-        }
-        q->gab = Lease<double>(c->pool, std::max<size_t>(q->runs.size(), 1) * 2 * maxnstep);
-        CK(cudaMemsetAsync(q->gab.p, 0, sizeof(double) * std::max<size_t>(q->runs.size(), 1) * 2 * maxnstep,
-                           c->stream));
-        q->phase = 3;
-    }
-    CKLAUNCH();
-    if (!green.empty()) {                                     // continued fractions of all finishing requests
-        std::vector<CFJob> cj;
-        std::vector<std::pair<ServReq*, int>> cjr;
-        size_t ng = 0;
-        for (ServReq* q : green) ng += q->runs.size();
-        Lease<double> g(c->pool, std::max<size_t>(ng, 1) * 2 * nw);
-        CK(cudaMemsetAsync(g.p, 0, sizeof(double) * std::max<size_t>(ng, 1) * 2 * nw, c->stream));
-        size_t gi = 0;
-        for (ServReq* q : green)
-            for (size_t r = 0; r < q->runs.size(); r++, gi++) {
-                GreenRun& gr = q->runs[r];
-                if (gr.nstep < 0) {
-                    const JobSpec& j = specs[-1 - gr.nstep];
-                    gr.nstep = j.nstep;
-                    gr.norm0 = j.norm0;
-                }
-                if (gr.nstep < 1) continue;
-                CFJob J;
-                J.a = gr.a; J.b = gr.b;
-                J.b1 = gr.norm0;
-                J.levels = (gr.nstep == 1 && maxnstep >= 2) ? 2 : gr.nstep;
-                J.zr_shift = (gr.pm == 1) ? gr.e0 : -gr.e0;
-                J.sign = (gr.pm == 1) ? -1.0 : 1.0;
-                J.g = g.p + gi * 2 * nw;
-                cj.push_back(J);
+    std::vector<std::vector<double>> gs(ng), abs_(ng);
+    for (size_t r = 0; r < ng; r++) gs[r].assign(hg.begin() + r * 2 * nw, hg.begin() + (r + 1) * 2 * nw);
+    const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
+    q.G.assign((size_t)2 * nw * I.model.norb * I.nspin, 0.0);
+    assemble_cluster(I.model.norb, I.nspin, even, maxnstep, nw, gs, abs_, 0, q.G.data(), nullptr);
+    q.jobs.clear();
+    q.phase = 4;
+}
+
+// One step: admit what fits, then serve the next size class in turn.
+int server_step(edzt_server* sv)
+{
+    edzt_ctx* c = sv->c;
+    server_admit(sv);
+    for (auto& up : sv->active)                               // cancelled requests leave now
+        if (up->cancelled) { up->error = "cancelled"; up->jobs.clear(); up->phase = 4; }
+    std::vector<int> classes;
+    for (auto& up : sv->active)
+        if (up->phase < 4) classes.push_back(up->cls);
+    std::sort(classes.begin(), classes.end());
+    classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
+    if (!classes.empty()) {
+        auto it = std::upper_bound(classes.begin(), classes.end(), sv->last_cls);
+        const int cls = (it == classes.end()) ? classes.front() : *it;
+        sv->last_cls = cls;
+        double left = sv->step_ms;
+        for (int round = 0; round < 64; round++) {
+            std::vector<LiveJob*> v;
+            long long dims = 0;
+            for (auto& up : sv->active) {
+                if (up->cls != cls || up->phase >= 4) continue;
+                for (auto& j : up->jobs)
+                    if (!j->done) { v.push_back(j.get()); dims += j->S.dim; }
             }
-        if (!cj.empty()) {
-            Lease<CFJob> dj(c->pool, cj.size());
-            CK(cudaMemcpyAsync(dj.p, cj.data(), sizeof(CFJob) * cj.size(), cudaMemcpyHostToDevice, c->stream));
-            launch_cf(dj.p, (int)cj.size(), sv->omega->as<double>(), nw, c->stream);
-            c->launches += 1;
-            CKLAUNCH();
-        }
-        std::vector<double> hg(std::max<size_t>(ng, 1) * 2 * nw);
-        CK(cudaMemcpyAsync(hg.data(), g.p, sizeof(double) * hg.size(), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        gi = 0;
-        for (ServReq* q : green) {
-            BatchInst& I = q->I;
-            std::vector<std::vector<double>> gs(q->runs.size()), abs_(q->runs.size());
-            for (size_t r = 0; r < q->runs.size(); r++, gi++)
-                gs[r].assign(hg.begin() + gi * 2 * nw, hg.begin() + (gi + 1) * 2 * nw);
-            const bool even = !(I.nspin == 2 || I.gs_up != I.gs_dn);
-            q->G.assign((size_t)2 * nw * I.model.norb * I.nspin, 0.0);
-            assemble_cluster(I.model.norb, I.nspin, even, maxnstep, nw, gs, abs_, 0, q->G.data(), nullptr);
-            q->phase = 4;
+            if (v.empty()) break;
+            auto est = sv->ms_per_phase.find(cls);
+            const double mpp = (est != sv->ms_per_phase.end()) ? est->second : 0.01 + (double)dims * 40.0 / 4.0e9;
+            int phases = (int)std::min(4096.0, std::max(2.0, left / std::max(mpp, 1e-4)));
+            phases &= ~1;
+            if (phases < 2) phases = 2;
+            const float ms = run_slice(c, v, phases);
+            const double per = ms / phases;
+            sv->ms_per_phase[cls] = (est != sv->ms_per_phase.end()) ? 0.5 * (est->second + per) : per;
+            left -= ms;
+            for (auto& up : sv->active) {                     // requests move on as their phase's runs finish
+                if (up->cls != cls || up->phase >= 4 || !phase_done(*up)) continue;
+                if (up->phase == 1) after_scan(sv, *up);
+                else if (up->phase == 2) after_eigvec(sv, *up);
+                else if (up->phase == 3) after_green(sv, *up);
+            }
+            if (left <= 0.0) break;
         }
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -1868,6 +2013,7 @@ int server_step(edzt_server* sv)
     for (auto it = sv->active.begin(); it != sv->active.end();) {
         if ((*it)->phase == 4) {
             ServReq& q = **it;
+            q.jobs.clear();
             q.I.gsvec.reset(); q.I.mt.reset(); q.ab.reset(); q.coef.reset(); q.gab.reset();
             sv->reserved -= q.I.footprint;
             sv->finished[q.id] = std::move(*it);
@@ -2084,8 +2230,9 @@ int edzt_hx(edzt_ctx* c, int ne_up, int ne_dn, const double* x, double* y, int a
         InVec xi(c, x, S.dim);
         OutVec yo(c, y, S.dim);
         if (accumulate) yo.preload();
-        launch_hx(S, xi.d, yo.d, accumulate ? 1 : 0, c->stream);
-        c->launches += 1;
+        Lease<double> hs(c->pool, (size_t)std::max(S.dim, 1LL));
+        launch_hx(S, xi.d, yo.d, accumulate ? 1 : 0, hs.p, c->stream);
+        c->launches += 2;
         CKLAUNCH();
         yo.finish();
         CK(cudaStreamSynchronize(c->stream));
@@ -2337,6 +2484,15 @@ int edzt_server_step(edzt_server* sv, int* nactive, int* nqueued, int* nfinished
         if (nfinished) *nfinished = nf;
         if (nactive) *nactive = (int)sv->active.size();
         if (nqueued) *nqueued = (int)sv->queue.size();
+    });
+}
+
+int edzt_server_set_step_ms(edzt_server* sv, double ms)
+{
+    if (!sv) return EDZT_ERR_ARG;
+    return guarded(sv->c, [&] {
+        arg_check(ms > 0.0 && std::isfinite(ms), "step time budget must be a positive number of ms");
+        sv->step_ms = ms;
     });
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 #include <atomic>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 #include "edzt_device.cuh"
 
@@ -43,8 +44,10 @@ void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32
 int edzt_max_hops(const DevModel& m, int sigma, int n);
 
 // ---- kernels.cu: standalone (non-persistent) kernels ------------------------
-int hx_rows_per_tile(int nup, int ndn, int hw_dn);
-void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s);
+// H.v in two phases (hv_phase.cuh); scratch: dim doubles of device memory.
+void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, double* scratch, cudaStream_t s);
+// Whether a sector's staged row and column slab fit in shared memory.
+bool hx_fits(int nup, int ndn);
 // Deterministic dot product: result written to *out (device).  partials needs
 // dot_partials_size() doubles.
 int dot_partials_size();
@@ -96,11 +99,38 @@ void launch_rl_div(double* out, const double* w, double beta, long long n, cudaS
 enum LzMode { LZ_COEFF = 0, LZ_EIGVEC = 1 };
 enum LzInit { LZ_INIT_HASH = 0, LZ_INIT_APPLYC = 1, LZ_INIT_COPY = 2 };
 
-// The Lanczos vectors of a run live as interleaved (y, w) pairs: y_k = H w_k
-// - b_k w_{k-1} and w_k, read and written together (one 16-byte access).
+// The tiles of one job in one phase (0: column phase, 1: row phase): tiles
+// [tile0, tile0 + ntiles) of that phase's list; its participants are CTAs
+// (tile0 + q) mod G, q < npart, and participant q owns partial-sum slot
+// slot0 + q.
+struct LzPhase {
+    long long tile0;
+    long long slot0;
+    int ntiles;
+    int npart;
+    int width;            // columns per slab (column phase) or rows per tile (row phase)
+    int pad;
+};
+
+// Recurrence state of one run between phases (every participating CTA
+// derives the same value; the first participant also stores it).
+struct LzState {
+    int k;                // the step in progress: opened by a column phase, finished by the row phase
+    int active;           // 1 while the run is going
+    int nstep;            // result: number of valid Lanczos steps
+    int opened;           // step k already opened (a_{k-1} derived) by the closing pass of a slice
+    double a_prev;        // a_{k-1}
+    double b_cur;         // b_k, the normaliser of the step (||v_init|| for k = 1)
+    double norm0;         // ||v_init||
+    double spare;
+};
+
+// The Lanczos vectors of a run live as interleaved pairs (y_k, w_k), one
+// 16-byte access each: step k writes YW[k & 1] and reads YW[(k - 1) & 1].
 struct LzJob {
     DevSector S;
     double2* YW[2];       // ping-pong pair buffers [dim]
+    double* D;            // [dim] down-hop part of H v_k, column phase -> row phase
     double* eig;          // EIGVEC: output eigenvector (unnormalised)
     const double* coeff;  // EIGVEC: ground eigenvector of the tridiagonal [nstep]
     double* a;            // [maxnstep] a(1..), written as steps are accepted
@@ -108,52 +138,55 @@ struct LzJob {
     int maxnstep;         // COEFF: LanczosSteps; EIGVEC: nstep of the coefficient pass
     int mode;
     int init;
-    int rows;             // rows per tile (full rows, staged in shared memory)
-    int ntiles;
-    int npart;            // participating CTAs = min(grid, ntiles)
-    long long tile0;      // first tile of this job in the global tile list
-    long long slot0;      // first of the job's npart partial-sum slots
+    int pad;
+    LzPhase ph[2];
+    LzState* st;          // [2] the run's state by phase parity (kept across launches of a sliced run)
     uint64_t key;         // LZ_INIT_HASH
     ApplyCArgs ac;        // LZ_INIT_APPLYC
     const double* src;    // LZ_INIT_APPLYC: the ground state; LZ_INIT_COPY: the start vector
-};
-
-// Recurrence state of one run between passes (every participating CTA
-// derives the same value; the first participant also stores it).
-struct LzState {
-    int k;                // step the pass computes (1-based); 0 before the first step
-    int active;           // 1 while the run is going
-    int nstep;            // result: number of valid Lanczos steps
-    int retry;            // the pass repeats step k with a corrected b_k
-    double a_prev;        // a_{k-1}
-    double b_cur;         // b_k, the normaliser of the step
-    double norm0;         // ||v_init||
-    double spare;
 };
 
 struct LzBatch {
     int njobs;
     int grid;
     int block;
-    int max_passes;
+    int max_phases;               // phase budget of the launch (even for a slice)
     size_t smem;
-    long long total_tiles;
+    long long total[2];           // tiles of the column and the row phase
     unsigned long long wait_ns;   // grid-barrier wait limit (0: the default 5 s)
     int stall_cta;                // fault test: this CTA leaves without arriving (-1: none)
+    int slice;                    // 1: a slice of longer runs; at the end of the budget every run
+                                  // still going opens its next step, so a later launch resumes it
 };
 
-int lz_grid_size(int device, size_t smem, int* block_out);
-// state: [njobs][2] (pass parity); partials: [slots][2][4]
-cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, LzState* state,
-                                      const long long* tile_prefix, double* partials,
+// Largest dynamic shared memory of one persistent CTA.
+constexpr size_t kLzSmemMax = 220 * 1024;
+// CTAs of block threads that can be resident with smem bytes each.
+int lz_grid_size(int device, size_t smem, int block);
+// jobs[j].st: the job's state by phase parity; prefix: [2][njobs + 1] tile
+// prefix sums of the column and row phases; slots: [slots][2] partial sums
+// by step parity.
+cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, const long long* prefix, double* slots,
                                       unsigned* sync_words, int* status, cudaStream_t s);
-// Rows per tile and the shared memory a tile of that many rows needs.
-int lz_rows_per_tile(int nup, int ndn, int hw_dn);
-// Rows per tile (<= rows_max) that spread a job of ndn rows evenly over G CTAs.
-int lz_rows_balanced(int ndn, int rows_max, int G);
-size_t lz_smem_bytes(int nup, int hw_dn, int rows);
+// Shared memory of a row tile of R rows, of a column slab of WC columns, and
+// of the fixed tables.
+size_t lz_row_smem(int nup, int R);
+size_t lz_col_smem(int ndn, int WC);
+size_t lz_fixed_smem();
 // Sync-word buffer size (bytes) for a grid of G CTAs.
 size_t lz_sync_bytes(int G);
+// Tile shapes of the jobs of one launch: every job's rows per tile and
+// columns per slab, the launch's block size, grid and shared memory; the
+// phases' tile lists, participants and slots are filled in.
+struct LzPlan {
+    int block = 256;
+    int grid = 0;
+    size_t smem = 0;
+    long long total[2] = {0, 0};
+    long long slots = 0;
+};
+LzPlan lz_plan(int device, LzJob* jobs, int njobs, std::vector<long long>& prefix);
+
 // ---- edzt_host.cu: context accessors (no table building, no allocation) -----
 struct edzt_ctx;
 int edzt_ctx_device(const edzt_ctx* c);

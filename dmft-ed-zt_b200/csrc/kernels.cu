@@ -3,9 +3,8 @@
 // continued fractions.  The fused persistent Lanczos lives in lanczos.cu.
 #include <cuda_runtime.h>
 #include "edzt_internal.h"
-#include "hv_row.cuh"
+#include "hv_phase.cuh"
 
-static constexpr size_t kHxSmemTarget = 24 * 1024;
 static constexpr int kWintDoubles = EDZT_MAX_P * EDZT_MAX_P;
 static constexpr int kAmpDoubles = EDZT_MAX_AMP;
 
@@ -16,94 +15,185 @@ int kernels_debug_bad(long long* out4)
 }
 #endif
 
-int hx_rows_per_tile(int nup, int ndn, int hw_dn)
-{
-    const size_t row = staged_row_bytes(nup, hw_dn);
-    int r = (int)(kHxSmemTarget / row);
-    if (r < 1) r = 1;
-    if (r > ndn) r = ndn;
-    return r;
-}
-
 // ---------------------------------------------------------------------------
 // H.v: y = H x (accumulate = 0) or y = y + H x (accumulate = 1), the `py`
-// flag of src/impurity_hamiltonian.f90:241-245.  One CTA per block of R full
-// rows; the rows and their per-row hop data are staged in shared memory.
-// T threads per CTA: 256, or for large sectors 512 (two CTAs per SM) and
-// 1024 (one), both at 64 registers, 32 warps per SM.
+// flag of src/impurity_hamiltonian.f90:241-245, in the two phases of
+// hv_phase.cuh: k_hx_col writes the down-hop part of every element into a
+// scratch vector D, then k_hx_row adds the diagonal, up-hop and exchange
+// parts.  Both stream their data once; all neighbour values come from
+// shared memory.
 // ---------------------------------------------------------------------------
-template <bool ACC, int T>
-__global__ void __launch_bounds__(T, T == 512 ? 2 : 1) k_hx(DevSector S, const double* __restrict__ x,
-                                                           double* __restrict__ y, int R)
+static constexpr int kHxThreads = 256;
+static constexpr size_t kHxSmemSoft = 100 * 1024;    // two CTAs per SM
+static constexpr size_t kHxSmemHard = 210 * 1024;    // one CTA per SM
+
+// Column phase: CTA b stages columns [b*WC, b*WC + WC) of every row.
+template <int WC>
+__global__ void __launch_bounds__(kHxThreads) k_hx_col(DevSector S, const double* __restrict__ x,
+                                                      double* __restrict__ D)
 {
+    constexpr int WS = phase_stride(WC);
+    extern __shared__ __align__(16) double smem[];
+    double* amp = smem;                                    // down-hop amplitudes
+    double* ws = smem + kAmpDoubles;                       // [ndn][WS]
+    const int nup = S.up.count, ndn = S.dn.count;
+    const int c0 = blockIdx.x * WC;
+    stage_table(S.dn.amp, S.dn.namp, amp);
+    const int n = ndn * WC;
+    for (int i0 = threadIdx.x; i0 < n; i0 += 4 * blockDim.x) {
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = i0 + q * blockDim.x;
+            const int id = i / WC, c = i - id * WC;
+            v[q] = (i < n && c0 + c < nup) ? __ldg(x + (size_t)id * nup + c0 + c) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = i0 + q * blockDim.x;
+            const int id = i / WC, c = i - id * WC;
+            if (i < n) ws[id * WS + c] = v[q];
+        }
+    }
+    __syncthreads();
+    for (int id = threadIdx.x; id < ndn; id += blockDim.x) {
+        double d[WC];
+        col_part<WC, WS>(S, ws, amp, id, d);
+        double* out = D + (size_t)id * nup + c0;
+#pragma unroll
+        for (int c = 0; c < WC; c++)
+            if (c0 + c < nup) out[c] = d[c];
+    }
+}
+
+// Row phase: CTA b stages rows [b*R, b*R + R), thread per column.
+template <bool ACC, int R>
+__global__ void __launch_bounds__(kHxThreads) k_hx_row(DevSector S, const double* __restrict__ x,
+                                                      const double* __restrict__ D, double* __restrict__ y)
+{
+    constexpr int RS = phase_stride(R);
     extern __shared__ __align__(16) double smem[];
     double* wint = smem;
     double* amp = smem + kWintDoubles;
+    double* xs = amp + kAmpDoubles;                        // [nup][RS]
     const int nup = S.up.count, ndn = S.dn.count;
-    Chunk C = chunk_layout(smem + kWintDoubles + kAmpDoubles, R, nup, S.dn.hw);
     const int r0 = blockIdx.x * R;
-    const int rows = min(R, ndn - r0);
-    const int n = rows * nup;
-    const long long g0 = (long long)r0 * nup;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) C.xs[e] = __ldg(x + g0 + e);
-    stage_rows(S.dn, C, r0, rows);
-    stage_wint(S, wint);
-    stage_amp(S.up, amp);
+    const int nr = min(R, ndn - r0);
+    stage_table(S.wint, S.P * S.P, wint);
+    stage_table(S.up.amp, S.up.namp, amp);
+    for (int iu = threadIdx.x; iu < nup; iu += blockDim.x) {
+        double v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = (r < nr) ? __ldg(x + (size_t)(r0 + r) * nup + iu) : 0.0;
+#pragma unroll
+        for (int r = 0; r < R; r++) xs[iu * RS + r] = v[r];
+    }
+    double e1d[R];
+    int pd[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int id = min(r0 + r, ndn - 1);
+        e1d[r] = __ldg(S.dn.e1 + id);
+        pd[r] = __ldg(S.dn.imp + id);
+    }
     __syncthreads();
     auto fetch = [&](long long idx) {
         EDZT_OK_OR(idx >= 0 && idx < S.dim, 61, idx, S.dim, blockIdx.x, return 0.0)
         return __ldg(x + idx);
     };
-    const SrcVec src{x};
-    int r = threadIdx.x / nup, iu = threadIdx.x - r * nup;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-        double du, dn;
-        hv_elem(S, C, wint, amp, src, r, iu, C.xs[e], du, dn);
-        double acc = du + dn;
-        if (S.has_j) acc = hv_exchange(S, C, r, iu, acc, fetch);
-        const long long g = g0 + e;
-        y[g] = ACC ? y[g] + acc : acc;
-        iu += blockDim.x;
-        while (iu >= nup) { iu -= nup; ++r; }
+    for (int iu = threadIdx.x; iu < nup; iu += blockDim.x) {
+        double acc[R];
+        row_part<R, RS>(S, xs, wint, amp, iu, e1d, pd, acc);
+        const int pu = S.has_j ? (int)__ldg(S.up.imp + iu) : 0;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            if (r >= nr) break;
+            const size_t g = (size_t)(r0 + r) * nup + iu;
+            double v = acc[r] + __ldg(D + g);
+            if (S.has_j) v = exchange_part(S, r0 + r, iu, pu, pd[r], v, fetch);
+            y[g] = ACC ? y[g] + v : v;
+        }
     }
 }
 
-// Threads per CTA of k_hx by sector dimension.  Measured on B200 (y = H x on
-// the half-filled sector of a single-orbital impurity): at nsite 16 (1.66e8
-// states) 4.45 / 3.10 / 2.85 ms with 256 / 512 / 1024 threads, at nsite 14
-// (1.18e7) 0.228 / 0.212 / 0.254 ms, at nsite 12 (8.5e5) 0.039 / 0.040 /
-// 0.042 ms.  Large sectors wait on the latency of their down-hop gathers,
-// which more warps per SM hide; small ones have too few row tiles to fill
-// 148 SMs with large CTAs.
-int hx_threads(long long dim)
+// Rows per tile: the most (of 8, 4, 2, 1) that fit two CTAs per SM and still
+// give every SM two tiles; columns per slab likewise (16, 8, 4, 2).  A
+// sector too large for that takes one CTA per SM.
+static int hx_rows_of(int nup, int ndn, int nsm)
 {
-    return dim >= (32LL << 20) ? 1024 : dim >= (4LL << 20) ? 512 : 256;
+    const int opts[4] = {8, 4, 2, 1};
+    for (int R : opts) {
+        const size_t sm = (kWintDoubles + kAmpDoubles + (size_t)nup * phase_stride(R)) * sizeof(double);
+        if (sm <= kHxSmemSoft && (ndn + R - 1) / R >= 2 * nsm) return R;
+    }
+    for (int R : {2, 1}) {
+        const size_t sm = (kWintDoubles + kAmpDoubles + (size_t)nup * phase_stride(R)) * sizeof(double);
+        if (sm <= kHxSmemSoft) return R;
+    }
+    return 1;
 }
 
-template <int T>
-static void launch_hx_t(const DevSector& S, const double* x, double* y, int accumulate, int tiles, int R,
-                        size_t smem, cudaStream_t s)
+static int hx_cols_of(int nup, int ndn, int nsm)
+{
+    const int opts[4] = {16, 8, 4, 2};
+    for (int W : opts) {
+        const size_t sm = (kAmpDoubles + (size_t)ndn * phase_stride(W)) * sizeof(double);
+        if (sm <= kHxSmemSoft && (nup + W - 1) / W >= 2 * nsm) return W;
+    }
+    return 2;
+}
+
+bool hx_fits(int nup, int ndn)
+{
+    const size_t row = (kWintDoubles + kAmpDoubles + (size_t)nup * phase_stride(1)) * sizeof(double);
+    const size_t col = (kAmpDoubles + (size_t)ndn * phase_stride(2)) * sizeof(double);
+    return row <= kHxSmemHard && col <= kHxSmemHard;
+}
+
+template <int R>
+static void launch_hx_row(const DevSector& S, const double* x, const double* D, double* y, int accumulate,
+                          cudaStream_t s)
 {
     static std::atomic<unsigned long long> attr_set{0};
     if (edzt_once_per_device(attr_set)) {
-        cudaFuncSetAttribute(k_hx<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        cudaFuncSetAttribute(k_hx<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_hx_row<false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
+        cudaFuncSetAttribute(k_hx_row<true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
     }
-    if (accumulate) k_hx<true, T><<<tiles, T, smem, s>>>(S, x, y, R);
-    else k_hx<false, T><<<tiles, T, smem, s>>>(S, x, y, R);
+    const int tiles = (S.dn.count + R - 1) / R;
+    const size_t sm = (kWintDoubles + kAmpDoubles + (size_t)S.up.count * phase_stride(R)) * sizeof(double);
+    if (accumulate) k_hx_row<true, R><<<tiles, kHxThreads, sm, s>>>(S, x, D, y);
+    else k_hx_row<false, R><<<tiles, kHxThreads, sm, s>>>(S, x, D, y);
 }
 
-void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s)
+template <int W>
+static void launch_hx_col(const DevSector& S, const double* x, double* D, cudaStream_t s)
+{
+    static std::atomic<unsigned long long> attr_set{0};
+    if (edzt_once_per_device(attr_set))
+        cudaFuncSetAttribute(k_hx_col<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
+    const int slabs = (S.up.count + W - 1) / W;
+    const size_t sm = (kAmpDoubles + (size_t)S.dn.count * phase_stride(W)) * sizeof(double);
+    k_hx_col<W><<<slabs, kHxThreads, sm, s>>>(S, x, D);
+}
+
+void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, double* scratch, cudaStream_t s)
 {
     const int nup = S.up.count, ndn = S.dn.count;
     if (nup <= 0 || ndn <= 0) return;
-    const int R = hx_rows_per_tile(nup, ndn, S.dn.hw);
-    const int tiles = (ndn + R - 1) / R;
-    const size_t smem = (kWintDoubles + kAmpDoubles) * sizeof(double) + (size_t)R * staged_row_bytes(nup, S.dn.hw);
-    switch (hx_threads(S.dim)) {
-    case 1024: launch_hx_t<1024>(S, x, y, accumulate, tiles, R, smem, s); break;
-    case 512: launch_hx_t<512>(S, x, y, accumulate, tiles, R, smem, s); break;
-    default: launch_hx_t<256>(S, x, y, accumulate, tiles, R, smem, s); break;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    switch (hx_cols_of(nup, ndn, nsm)) {
+    case 16: launch_hx_col<16>(S, x, scratch, s); break;
+    case 8: launch_hx_col<8>(S, x, scratch, s); break;
+    case 4: launch_hx_col<4>(S, x, scratch, s); break;
+    default: launch_hx_col<2>(S, x, scratch, s); break;
+    }
+    switch (hx_rows_of(nup, ndn, nsm)) {
+    case 8: launch_hx_row<8>(S, x, scratch, y, accumulate, s); break;
+    case 4: launch_hx_row<4>(S, x, scratch, y, accumulate, s); break;
+    case 2: launch_hx_row<2>(S, x, scratch, y, accumulate, s); break;
+    default: launch_hx_row<1>(S, x, scratch, y, accumulate, s); break;
     }
 }
 

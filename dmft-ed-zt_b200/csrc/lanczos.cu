@@ -2,86 +2,64 @@
 //
 // One cooperative launch runs every step of many independent Lanczos runs
 // ("jobs": sectors of the ground-state search, the eigenvector pass of the
-// winning sector, c / c^+ excitation runs of the Green's function).  Each
-// job is cut into tiles of whole rows; the tiles of all jobs form one list
-// and CTA b takes tiles b, b+G, b+2G, ... in every pass, so the CTAs sweep
-// the vectors together (the rows a sweep gathers from stay in L2) and the
-// same CTAs meet the same job every pass.  Passes are separated by a
-// hierarchical grid barrier with a bounded wait.
+// winning sector, c / c^+ excitation runs of the Green's function).
 //
 // The recurrence is the reference's (src/lanczos_solver.f90:92-173):
-//   w_k = v_k / b_k,  v_k = y_{k-1} - a_{k-1} w_{k-1},
-//   y_k = H w_k - b_k w_{k-1},  a_k = <w_k, y_k>,  b_{k+1} = ||y_k - a_k w_k||.
-// Fusion: a pass stores the pair (y_k, w_k); the next pass forms w_{k+1}
-// wherever it reads it (rows staged in shared memory for the up-spin hops,
-// down-spin neighbours gathered as one 16-byte pair per hop), so a step is
-// one sweep.  Its sums are taken around the shift a_{k-1}: with
-// t = y - a_{k-1} w it reduces <w,t>, <t,t>, <w,w>, so a_k = a_{k-1}<w,w> +
-// <w,t> and, with d = a_k - a_{k-1}, b_{k+1}^2 = <t,t> - 2d<w,t> + d^2<w,w>.
-// The next pass, which forms v_{k+1} element by element anyway, also sums
-// ||v_{k+1}||^2 exactly; when that disagrees with the b_{k+1} it used (by
-// more than 1e-12 relative, e.g. in an exhausted Krylov space of a tiny
-// sector) the job repeats that step with the exact norm, as the reference
-// computes it.  The first step divides v_init by its norm exactly as the
-// reference does, so a one-dimensional sector breaks down with b(2) = 0.
+//   v_1 = v_init,  v_k = y_{k-1} - a_{k-1} w_{k-1}  (k >= 2),
+//   b_k = ||v_k||,  w_k = v_k / b_k,
+//   y_k = H w_k - b_k w_{k-1},  a_k = <w_k, y_k>,
+// with a(1..), b(1) = 0, b(k) = ||v_k|| (k >= 2) stored as they are accepted.
 //
-// Between passes every participating CTA of a job re-derives the job's
-// scalars from the partial sums of the previous pass (slots in a fixed order,
-// so all of them get the same bits) and the first participant also stores
-// them; partial sums and states are double-buffered by pass parity, so no
-// per-job atomics are needed.
-#include <cuda_runtime.h>
+// A step is two phases of the whole grid, separated by grid barriers; H.v
+// is split as in hv_phase.cuh:
+//   column phase  each CTA stages slabs of whole columns of v_k (formed from
+//                 the stored pair (y_{k-1}, w_{k-1}) element by element),
+//                 sums ||v_k||^2 exactly and writes D = the down-hop part of
+//                 H v_k (not yet normalised);
+//   row phase     with b_k known from those sums, each CTA stages tiles of
+//                 whole rows of w_k = v_k / b_k, adds the diagonal, up-hop and
+//                 exchange parts to D / b_k, subtracts b_k w_{k-1}, stores the
+//                 pair (y_k, w_k) and sums <w_k, y_k> exactly.
+// Every neighbour value comes from shared memory, every global access is a
+// coalesced stream (pair buffers, D, the eigenvector), and both reductions
+// are exact sums, as in the reference.  The tiles of all jobs of a phase
+// form one list; CTA b takes tiles b, b+G, ... in every phase, and each
+// job's participants in a phase write one partial sum each into their slot
+// (double-buffered by step parity).  Every participating CTA re-derives a
+// job's scalars from the slots in a fixed order, so all of them get the same
+// bits; the first participant also stores them.
+//
+// The eigenvector pass (LZ_EIGVEC) reruns the recurrence with the stored
+// a, b (src/lanczos_solver.f90:213-300) and accumulates sum_k coeff_k w_k.
+//
+// A launch may be a slice of longer runs (LzBatch::slice): when its phase
+// budget runs out, a closing pass opens every unfinished run's next step
+// (derives a(k-1) and the finish test) and stores the state marked opened,
+// so a later launch, with any mix of other runs, resumes it.
+#include <algorithm>
 #include <type_traits>
+#include <cuda_runtime.h>
 #include "edzt_internal.h"
-#include "hv_row.cuh"
+#include "hv_phase.cuh"
 
-static constexpr int kLzThreads = 256;
-// CTAs per SM the register allocation is sized for
-#ifndef EDZT_LZ_MINBLOCKS
-#define EDZT_LZ_MINBLOCKS 2
-#endif
-static constexpr size_t kLzTileTarget = 24 * 1024;
-static constexpr double kVerifyTol = 1.0e-12;
 static constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000ull * 1000ull * 1000ull;
-static constexpr int kFixedDoubles = 128 + EDZT_MAX_P * EDZT_MAX_P + EDZT_MAX_AMP;   // reduction scratch, wint, amp
-static constexpr int kBarGroup = 16;                                  // CTAs per barrier group
+static constexpr int kRedDoubles = 32;
+static constexpr int kWintDoubles = EDZT_MAX_P * EDZT_MAX_P;
+static constexpr int kFixedDoubles = kRedDoubles + kWintDoubles + 2 * EDZT_MAX_AMP;
+static constexpr int kBarGroup = 16;                    // CTAs per barrier group
 
 // sync words (unsigned), each counter on its own 128-byte line; SW_GEN is a
 // 64-bit word (barrier count << 32 | runs still going)
 #define SW_GEN 0
 #define SW_TOP 32
 #define SW_ACTIVE 64
-
 #define SW_GROUP(g) (128 + 32 * (g))
 
 size_t lz_sync_bytes(int G) { return sizeof(unsigned) * (128 + 32 * (size_t)((G + kBarGroup - 1) / kBarGroup)); }
 
-int lz_rows_per_tile(int nup, int ndn, int hw_dn)
-{
-    int r = (int)(kLzTileTarget / staged_row_bytes(nup, hw_dn));
-    if (r < 1) r = 1;
-    if (r > ndn) r = ndn;
-    return r;
-}
-
-int lz_rows_balanced(int ndn, int rows_max, int G)
-{
-    // rows per tile <= rows_max minimising the rows one CTA sweeps when the
-    // job runs alone, ceil(tiles / G) * rows; ties go to fewer, larger tiles
-    int best = rows_max;
-    long long best_cost = -1;
-    for (int r = rows_max; r >= 1; r--) {
-        const long long tiles = (ndn + r - 1) / r;
-        const long long cost = ((tiles + G - 1) / G) * r;
-        if (best_cost < 0 || cost < best_cost) { best = r; best_cost = cost; }
-    }
-    return best;
-}
-
-size_t lz_smem_bytes(int nup, int hw_dn, int rows)
-{
-    return kFixedDoubles * sizeof(double) + (size_t)rows * staged_row_bytes(nup, hw_dn);
-}
+size_t lz_row_smem(int nup, int R) { return 2 * (size_t)nup * phase_stride(R) * sizeof(double); }
+size_t lz_col_smem(int ndn, int WC) { return (size_t)ndn * phase_stride(WC) * sizeof(double); }
+size_t lz_fixed_smem() { return kFixedDoubles * sizeof(double); }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns()
 {
@@ -90,15 +68,6 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     return t;
 }
 
-// Hierarchical grid barrier with a bounded wait.  Counters only grow: the
-// k-th barrier of a launch is complete on a group counter at k * (group
-// size) arrivals and on the top counter at k * (number of groups), so no
-// counter is read before arriving or reset after.  CTAs arrive on the counter
-// of their group of 16, the last of each group on the top counter, and the
-// last of all publishes (k << 32 | runs still going) in the 64-bit
-// generation word, which the others wait for.  Returns false (and the kernel
-// stops) when the wait ran out or another CTA reported an error; *snap
-// receives the number of runs still going.
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p)
 {
     unsigned long long v;
@@ -111,6 +80,15 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Hierarchical grid barrier with a bounded wait.  Counters only grow: the
+// k-th barrier of a launch is complete on a group counter at k * (group
+// size) arrivals and on the top counter at k * (number of groups), so no
+// counter is read before arriving or reset after.  CTAs arrive on the counter
+// of their group of 16, the last of each group on the top counter, and the
+// last of all publishes (k << 32 | runs still going) in the 64-bit
+// generation word, which the others wait for.  Returns false (and the kernel
+// stops) when the wait ran out or another CTA reported an error; snap
+// receives the number of runs still going.
 __device__ bool grid_barrier(unsigned* sw, int* status, unsigned& nbar, unsigned& snap, const LzBatch& B)
 {
     if ((int)blockIdx.x == B.stall_cta) return false;   // fault test: leave without arriving
@@ -168,319 +146,319 @@ __device__ __forceinline__ int find_job(const long long* __restrict__ prefix, in
     return lo;
 }
 
-// ---------------------------------------------------------------------------
-// scalar recurrence between passes (same on every participating CTA)
-// ---------------------------------------------------------------------------
-struct Sums {
-    double wt, tt, ww, vv;
-};
-
-// State of the pass after `prev`, from the sums of the pass that used `prev`.
-// `out` marks the first participant: it stores a(k), b(k) as they are
-// accepted and counts finished runs.
-__device__ LzState advance(const LzJob& J, const LzState& prev, const Sums& s, bool out, unsigned* sw)
+// Element e of the start vector of a job.
+__device__ __forceinline__ double init_value(const LzJob& J, long long e)
 {
-    LzState n = prev;
-    n.retry = 0;
-    if (!prev.active) return n;
-    auto finish = [&](int nstep) {
-        n.active = 0;
-        n.nstep = nstep;
-        if (out) atomicSub(sw + SW_ACTIVE, 1u);
-    };
-    if (prev.k == 0) {                                  // after the start-vector pass
-        const double nrm = sqrt(s.vv);
-        n.norm0 = nrm;
-        if (!(nrm > 0.0)) { finish(0); return n; }      // zero start vector
-        n.k = 1;
-        n.a_prev = 0.0;
-        n.b_cur = nrm;
-        return n;
-    }
-    const int k = prev.k;
-    if (J.mode == LZ_EIGVEC) {                          // stored coefficients, no sums
-        if (k >= J.maxnstep) { finish(k); return n; }
-        n.k = k + 1;
-        n.a_prev = J.a[k - 1];
-        n.b_cur = J.b[k];
-        return n;
-    }
-    if (k >= 2) {                                       // verify the b_k the step used
-        const double bex = sqrt(s.vv);
-        if (bex < 1.0e-16) {                            // breakdown (lanczos_solver.f90:161)
-            if (out) J.b[k - 1] = 0.0;
-            finish(k - 1);
-            return n;
-        }
-        if (!(fabs(bex - prev.b_cur) <= kVerifyTol * bex)) {
-            if (out) J.b[k - 1] = bex;
-            n.b_cur = bex;
-            n.retry = 1;
-            return n;
-        }
-    }
-    const double ah = (k == 1) ? 0.0 : prev.a_prev;
-    const double a = fma(ah, s.ww, s.wt);               // a(k) = <w, y>  (lanczos_solver.f90:134,159)
-    if (out) {
-        J.a[k - 1] = a;
-        if (k == 1) J.b[0] = 0.0;                       // :135
-    }
-    if (k >= J.maxnstep) { finish(k); return n; }       // :137-141, :161-164
-    const double d = a - ah;
-    const double bb2 = s.tt - 2.0 * d * s.wt + d * d * s.ww;
-    // an ill-conditioned or non-positive estimate is repaired by the next
-    // pass's exact norm (one repeated step)
-    const double bn = sqrt(fmax(bb2, 1.0e-300));
-    if (out) J.b[k] = bn;
-    n.k = k + 1;
-    n.a_prev = a;
-    n.b_cur = bn;
-    return n;
+    if (J.init == LZ_INIT_HASH) return edzt_u01(J.key, (uint64_t)e);
+    if (J.init == LZ_INIT_APPLYC) return apply_c_value(J.ac, J.src, e);
+    return __ldg(J.src + e);
+}
+
+// v_k at element e: the start vector for k = 1, else y_{k-1} - a_{k-1} w_{k-1}
+// from the stored pair.  Every phase and every CTA forms it with this one
+// expression, so all get the same bits.
+__device__ __forceinline__ double form_v(const LzJob& J, int k, const double2* __restrict__ pin, double am,
+                                         long long e)
+{
+    if (k == 1) return init_value(J, e);
+    const double2 pr = __ldcg(pin + e);
+    return fma(am, pr.y, pr.x);
 }
 
 // ---------------------------------------------------------------------------
 // the persistent kernel
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kLzThreads, EDZT_LZ_MINBLOCKS)
-    k_lanczos(LzBatch B, const LzJob* __restrict__ jobs, LzState* __restrict__ state,
-              const long long* __restrict__ prefix, double* __restrict__ partials, unsigned* __restrict__ sw,
-              int* __restrict__ status)
+__global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restrict__ jobs,
+                                                 const long long* __restrict__ prefix, double* __restrict__ slots,
+                                                 unsigned* __restrict__ sw, int* __restrict__ status)
 {
     extern __shared__ __align__(16) double smem[];
-    double* red = smem;                                  // 128 doubles of reduction scratch
-    double* wint = smem + 128;                           // interaction energies by impurity patterns
-    double* amp = wint + EDZT_MAX_P * EDZT_MAX_P;        // up-spin hop amplitudes by slot
-    double* chunk_base = smem + kFixedDoubles;           // staged rows of the current tile
+    double* red = smem;                                  // reduction scratch
+    double* wint = red + kRedDoubles;                    // interaction energies by impurity patterns
+    double* amp_up = wint + kWintDoubles;                // up-spin hop amplitudes by slot
+    double* amp_dn = amp_up + EDZT_MAX_AMP;              // down-spin hop amplitudes by slot
+    double* chunk = smem + kFixedDoubles;                // the staged row tile or column slab
     __shared__ LzJob sJ;
     __shared__ LzState sS;
     __shared__ int s_job;
+    __shared__ int s_resumed;
 
     const int G = gridDim.x;
+    const int T = blockDim.x;
     unsigned nbar = 0u;                                  // grid barriers this CTA has passed
     if (threadIdx.x == 0) s_job = -1;
     __syncthreads();
 
-    // slot of this CTA in the current job (participants: CTAs (tile0 + q) mod G, q < npart)
-    auto my_q = [&]() { return (int)(((long long)blockIdx.x - sJ.tile0 % G + G) % G); };
+    // participant index of this CTA in phase ph of the current job
+    auto my_q = [&](int ph) { return (int)(((long long)blockIdx.x - sJ.ph[ph].tile0 % G + G) % G); };
 
-    // Enter job j in pass `pass`: load it if needed and derive its state.
-    auto begin_job = [&](int j, int pass) {
+    // Sum of the current job's partial-sum slots of phase ph at parity par,
+    // in participant order (every thread returns it).
+    auto slot_sum = [&](int ph, int par) {
+        double v[1] = {0.0};
+        for (int i = threadIdx.x; i < sJ.ph[ph].npart; i += T) v[0] += __ldcg(slots + (sJ.ph[ph].slot0 + i) * 2 + par);
+        block_sum<1>(v, red);
+        return v[0];
+    };
+
+    // Enter job j in phase p: load it if needed and derive its state.  The
+    // closing pass of a slice (closing) opens the next step only: it derives
+    // a(k-1) and the finish test of a column phase and stores the state,
+    // marked opened, under both parities for the launch that resumes it.
+    auto begin_job = [&](int j, int p, bool closing) {
         __syncthreads();
         if (j != s_job) {
             const int* src = reinterpret_cast<const int*>(jobs + j);
             int* dst = reinterpret_cast<int*>(&sJ);
-            for (int i = threadIdx.x; i < (int)(sizeof(LzJob) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
+            for (int i = threadIdx.x; i < (int)(sizeof(LzJob) / sizeof(int)); i += T) dst[i] = __ldg(src + i);
             __syncthreads();
-            stage_wint(sJ.S, wint);
-            stage_amp(sJ.S.up, amp);
+            stage_table(sJ.S.wint, sJ.S.P * sJ.S.P, wint);
+            stage_table(sJ.S.up.amp, sJ.S.up.namp, amp_up);
+            stage_table(sJ.S.dn.amp, sJ.S.dn.namp, amp_dn);
             if (threadIdx.x == 0) s_job = j;
         }
-        if (pass == 0) {
-            if (threadIdx.x == 0) {
-                const int* ss = reinterpret_cast<const int*>(state + 2 * (size_t)j);
-                int* sd = reinterpret_cast<int*>(&sS);
-                for (int i = 0; i < (int)(sizeof(LzState) / sizeof(int)); i++) sd[i] = __ldcg(ss + i);
-            }
+        const int ph = p & 1;
+        if (threadIdx.x == 0) {
+            const int* ss = reinterpret_cast<const int*>(sJ.st + ((p + 1) & 1));
+            int* sd = reinterpret_cast<int*>(&sS);
+            for (int i = 0; i < (int)(sizeof(LzState) / sizeof(int)); i++) sd[i] = __ldcg(ss + i);
+            s_resumed = (ph == 0 && sS.opened);          // step already opened by a closing pass
+            if (ph == 0 && !sS.opened) sS.k += 1;        // the column phase opens the next step
+            sS.opened = 0;
+        }
+        __syncthreads();
+        if (s_resumed) {
+            if (threadIdx.x == 0 && my_q(0) == 0) sJ.st[p & 1] = sS;
             __syncthreads();
             return;
         }
-        // sum the previous pass's slots in participant order
-        double v[4] = {0.0, 0.0, 0.0, 0.0};
-        const int par = (pass - 1) & 1;
-        for (int i = threadIdx.x; i < sJ.npart; i += blockDim.x) {
-            const double* p = partials + ((sJ.slot0 + i) * 2 + par) * 4;
-            v[0] += __ldcg(p); v[1] += __ldcg(p + 1); v[2] += __ldcg(p + 2); v[3] += __ldcg(p + 3);
-        }
-        block_sum<4>(v, red);
-        if (threadIdx.x == 0) {
-            LzState prev;
-            const int* ss = reinterpret_cast<const int*>(state + 2 * (size_t)j + par);
-            int* sd = reinterpret_cast<int*>(&prev);
-            for (int i = 0; i < (int)(sizeof(LzState) / sizeof(int)); i++) sd[i] = __ldcg(ss + i);
-            const bool first = (my_q() == 0);
-            Sums s{v[0], v[1], v[2], v[3]};
-            sS = advance(sJ, prev, s, first, sw);
-            if (first) state[2 * (size_t)j + (pass & 1)] = sS;   // published by the barrier's fence
-        }
-        __syncthreads();
-    };
-
-    auto flush = [&](int pass, double (&acc)[4]) {
-        block_sum<4>(acc, red);
-        if (threadIdx.x == 0) {
-            EDZT_OK_OR(my_q() < sJ.npart, 24, blockIdx.x, sJ.tile0, sJ.npart, return)
-            double* p = partials + ((sJ.slot0 + my_q()) * 2 + (pass & 1)) * 4;
-            p[0] = acc[0]; p[1] = acc[1]; p[2] = acc[2]; p[3] = acc[3];
-        }
-    };
-
-    // Start vector rows of tile tl: materialise (v, 0) pairs, sum v^2.
-    auto init_tile = [&](int tl, double (&acc)[4]) {
-        const int nup = sJ.S.up.count;
-        const int r0 = tl * sJ.rows, rows = min(sJ.rows, sJ.S.dn.count - r0);
-        const long long g0 = (long long)r0 * nup, n = (long long)rows * nup;
-        double2* Y1 = sJ.YW[1];
-        for (long long e = threadIdx.x; e < n; e += blockDim.x) {
-            const long long g = g0 + e;
-            EDZT_OK_OR(g < sJ.S.dim, 25, g, sJ.S.dim, tl, break)
-            double v;
-            if (sJ.init == LZ_INIT_HASH) v = edzt_u01(sJ.key, (uint64_t)g);
-            else if (sJ.init == LZ_INIT_APPLYC) v = apply_c_value(sJ.ac, sJ.src, g);
-            else v = __ldg(sJ.src + g);
-            __stcg(Y1 + g, make_double2(v, 0.0));
-            acc[3] = fma(v, v, acc[3]);
-        }
-    };
-
-    // One Lanczos step (k = sS.k) on the rows of tile tl.  The first step
-    // (FIRST) divides by the start vector's norm exactly; later steps
-    // multiply by 1/b_k, so no division sits in their loops.
-    auto step_tile = [&](auto first_tag, int tl, double (&acc)[4]) {
-        constexpr bool FIRST = decltype(first_tag)::value;
-        const int nup = sJ.S.up.count, hwd = sJ.S.dn.hw;
         const int k = sS.k;
-        const int p = k & 1;
-        const double2* __restrict__ YWp = sJ.YW[p];
-        double2* __restrict__ YWn = sJ.YW[p ^ 1];
-        const double b_cur = sS.b_cur, rb = 1.0 / b_cur, am = -sS.a_prev, mb = -b_cur;
         const bool coeff = (sJ.mode == LZ_COEFF);
-        const double ck = coeff ? 0.0 : sJ.coeff[k - 1];
-        auto fetch = [&](long long idx) {
-            EDZT_OK_OR(idx >= 0 && idx < sJ.S.dim, 21, idx, sJ.S.dim, k, return 0.0)
-            const double2 pr = __ldcg(YWp + idx);
-            if (FIRST) return pr.x / b_cur;
-            return fma(am, pr.y, pr.x) * rb;
-        };
-        const int r0 = tl * sJ.rows, rows = min(sJ.rows, sJ.S.dn.count - r0);
-        Chunk C = chunk_layout(chunk_base, sJ.rows, nup, hwd);
-        const int n = rows * nup;
-        EDZT_OK_OR(rows >= 1 && (long long)r0 * nup + n <= sJ.S.dim, 22, r0, rows, n, return)
-        const double2* __restrict__ Yt = YWp + (long long)r0 * nup;
-        double2* __restrict__ Ot = YWn + (long long)r0 * nup;
-        double* __restrict__ Et = coeff ? nullptr : sJ.eig + (long long)r0 * nup;
-        for (int e0 = threadIdx.x; e0 < n; e0 += 4 * blockDim.x) {
-            double2 pr[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int e = e0 + q * blockDim.x;
-                pr[q] = (e < n) ? __ldcg(Yt + e) : make_double2(0.0, 0.0);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int e = e0 + q * blockDim.x;
-                if (e >= n) break;
-                if (FIRST) {
-                    C.xs[e] = pr[q].x / b_cur;
-                } else {
-                    const double v = fma(am, pr[q].y, pr[q].x);
-                    acc[3] = fma(v, v, acc[3]);      // exact ||v_k||^2: verifies b_k
-                    C.xs[e] = v * rb;
-                }
-            }
-        }
-        stage_rows(sJ.S.dn, C, r0, rows);
-        __syncthreads();
-        // Warps take (row, column segment) items; a row's down hops, energy and
-        // impurity bits are loaded once per item into registers, and the warp
-        // walks its segment 32 columns at a time.
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-        const int W = max(32, ((nup + nwarps - 1) / nwarps + 31) & ~31);
-        const int nseg = (nup + W - 1) / W;
-        const uint4* __restrict__ hpk = sJ.S.up.hpk;
-        const bool two = sJ.S.up.hw > 4;
-        for (int item = warp; item < rows * nseg; item += nwarps) {
-            const int r = item / nseg, c0 = (item - r * nseg) * W, c1 = min(nup, c0 + W);
-            const int hd = C.dcnt[r];
-            EDZT_OK_OR(hd >= 0 && hd <= C.hw, 13, r, hd, C.hw, continue)
-            const DHop* __restrict__ rec = C.dh + r * C.hw;
-            unsigned off[8];                                         // amplitudes stay in shared memory
-#pragma unroll
-            for (int q = 0; q < 8; q++) off[q] = (q < hd) ? (unsigned)rec[q].off : 0u;
-            const double rowe = C.de1[r];
-            const double* __restrict__ wrow = wint + C.dimp[r];
-            const double* __restrict__ xrow = C.xs + r * nup;
-            for (int iu = c0 + lane; iu < c1; iu += 32) {
-                const int e = r * nup + iu;
-                const double2* __restrict__ col = YWp + iu;
-                // every load of the element first
-                const uint4 q0 = __ldg(hpk + iu);
-                const uint4 q1 = two ? __ldg(hpk + nup + iu) : make_uint4(0u, 0u, 0u, 0u);
-                const int hu = __ldg(sJ.S.up.hcnt + iu);
-                const int pu = __ldg(sJ.S.up.imp + iu);
-                const double e1u = __ldg(sJ.S.up.e1 + iu);
-                const double wprev = FIRST ? 0.0 : __ldcg(reinterpret_cast<const double*>(Yt + e) + 1);
-                const double eprev = (coeff || FIRST) ? 0.0 : __ldcg(Et + e);
-                double2 g[8];
-#pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    EDZT_OK_OR(q >= hd || (long long)off[q] + iu < sJ.S.dim, 21, off[q], iu, sJ.S.dim, g[q] = make_double2(0.0, 0.0); continue)
-                    g[q] = (q < hd) ? __ldcg(col + off[q]) : make_double2(0.0, 0.0);
-                }
-                // diagonal and up hops from the staged row
-                const double xe = xrow[iu];
-                double hv = (e1u + rowe + wrow[pu * sJ.S.P]) * xe;
-                const uint32_t eu[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-#pragma unroll
-                for (int c = 0; c < 8; c++) {
-                    if (c < hu) {
-                        EDZT_OK_OR(edzt_hop_rank(eu[c]) < nup && edzt_hop_slot(eu[c]) < sJ.S.up.namp, 11, iu, c,
-                                   (long long)eu[c], continue)
-                        hv = fma(amp[edzt_hop_slot(eu[c])], xrow[edzt_hop_rank(eu[c])], hv);
+        // sums needed: a(k-1) before a column phase, ||v_k||^2 before a row
+        // phase (the eigenvector pass takes a and b from the coefficient pass
+        // but sums ||v_init|| itself)
+        double sum = 0.0;
+        if (sS.active && ((ph == 0 && k >= 2 && coeff) || (ph == 1 && (coeff || k == 1))))
+            sum = (ph == 0) ? slot_sum(1, (k - 1) & 1) : slot_sum(0, k & 1);
+        if (threadIdx.x == 0) {
+            const bool out = (my_q(ph) == 0);
+            LzState n = sS;
+            auto finish = [&](int nstep) {
+                n.active = 0;
+                n.nstep = nstep;
+                if (out) atomicSub(sw + SW_ACTIVE, 1u);
+            };
+            if (n.active) {
+                if (ph == 0) {
+                    if (k >= 2) {                        // a(k-1) = <w, y> of the last row phase (:134,159)
+                        const double a = coeff ? sum : sJ.a[k - 2];
+                        if (out && coeff) sJ.a[k - 2] = a;
+                        n.a_prev = a;
+                        if (k - 1 >= sJ.maxnstep) finish(k - 1);          // :137-141, :161-164
+                    } else {
+                        n.a_prev = 0.0;
+                    }
+                } else if (k == 1) {                     // ||v_init|| (:128-130); b(1) = 0 (:135)
+                    const double nrm = sqrt(sum);
+                    n.norm0 = nrm;
+                    n.b_cur = nrm;
+                    if (out && coeff) sJ.b[0] = 0.0;
+                    if (!(nrm > 0.0)) finish(0);         // zero start vector
+                } else {                                 // b(k) = ||v_k|| (:144,167), breakdown (:161)
+                    const double bk = coeff ? sqrt(sum) : sJ.b[k - 1];
+                    if (coeff && bk < 1.0e-16) {
+                        if (out) sJ.b[k - 1] = 0.0;
+                        finish(k - 1);
+                    } else {
+                        if (out && coeff) sJ.b[k - 1] = bk;
+                        n.b_cur = bk;
                     }
                 }
-                for (int h0 = 8; h0 < hu; h0 += 4) {                 // hop lists longer than 8
-                    const uint4 q = __ldg(hpk + (size_t)(h0 >> 2) * nup + iu);
-                    const uint32_t f[4] = {q.x, q.y, q.z, q.w};
+            }
+            if (closing && n.active) n.opened = 1;
+            if (out) {                                   // published by the barrier's fence (or the launch's end)
+                sJ.st[p & 1] = n;
+                if (closing) sJ.st[(p + 1) & 1] = n;
+            }
+            sS = n;
+        }
+        __syncthreads();
+    };
+
+    auto flush = [&](int ph, double acc) {
+        double v[1] = {acc};
+        block_sum<1>(v, red);
+        if (threadIdx.x == 0) {
+            EDZT_OK_OR(my_q(ph) < sJ.ph[ph].npart, 24, blockIdx.x, sJ.ph[ph].tile0, sJ.ph[ph].npart, return)
+            slots[(sJ.ph[ph].slot0 + my_q(ph)) * 2 + (sS.k & 1)] = v[0];
+        }
+    };
+
+    // Column phase of step k on slab tl: stage v_k on columns [c0, c0 + WC)
+    // of every row, sum v^2, write the down-hop part of H v_k into D.
+    auto col_tile = [&](auto wc_tag, int tl, double& acc) {
+        constexpr int WC = decltype(wc_tag)::value;
+        constexpr int WS = phase_stride(WC);
+        const int nup = sJ.S.up.count, ndn = sJ.S.dn.count, k = sS.k;
+        const double2* __restrict__ pin = sJ.YW[(k + 1) & 1];
+        const double am = -sS.a_prev;
+        const int c0 = tl * WC;
+        double* ws = chunk;
+        const int n = ndn * WC;
+        for (int i0 = threadIdx.x; i0 < n; i0 += 4 * T) {
+            double v[4];
 #pragma unroll
-                    for (int c = 0; c < 4; c++)
-                        if (h0 + c < hu) hv = fma(amp[edzt_hop_slot(f[c])], xrow[edzt_hop_rank(f[c])], hv);
-                }
-                // down hops: v = y - a w at each neighbour, as its owner forms it
-                double dv = 0.0;
+            for (int q = 0; q < 4; q++) {
+                const int i = i0 + q * T;
+                const int id = i / WC, c = i - id * WC;
+                v[q] = (i < n && c0 + c < nup) ? form_v(sJ, k, pin, am, (long long)id * nup + c0 + c) : 0.0;
+            }
 #pragma unroll
-                for (int q = 0; q < 8; q++)
-                    if (q < hd) dv = fma(rec[q].val, fma(am, g[q].y, g[q].x), dv);
-                for (int h = 8; h < hd; h++) {
-                    const double2 gg = __ldcg(col + rec[h].off);
-                    dv = fma(rec[h].val, fma(am, gg.y, gg.x), dv);
+            for (int q = 0; q < 4; q++) {
+                const int i = i0 + q * T;
+                const int id = i / WC, c = i - id * WC;
+                if (i < n) {
+                    ws[id * WS + c] = v[q];
+                    acc = fma(v[q], v[q], acc);
                 }
-                hv += FIRST ? dv / b_cur : dv * rb;                   // sum c * w_k(id', iu)
-                if (sJ.S.has_j) hv = hv_exchange(sJ.S, C, r, iu, hv, fetch);
-                const double y = FIRST ? hv : fma(mb, wprev, hv);
-                __stcg(Ot + e, make_double2(y, xe));
+            }
+        }
+        __syncthreads();
+        for (int id = threadIdx.x; id < ndn; id += T) {
+            double d[WC];
+            col_part<WC, WS>(sJ.S, ws, amp_dn, id, d);
+            double* out = sJ.D + (long long)id * nup + c0;
+#pragma unroll
+            for (int c = 0; c < WC; c++)
+                if (c0 + c < nup) __stcg(out + c, d[c]);
+        }
+        __syncthreads();
+    };
+
+    // Row phase of step k on tile tl: stage w_k = v_k / b_k (and w_{k-1}) on
+    // rows [r0, r0 + R), finish y_k = H w_k - b_k w_{k-1}, store (y_k, w_k),
+    // sum <w_k, y_k> (or accumulate the eigenvector).
+    auto row_tile = [&](auto r_tag, int tl, double& acc) {
+        constexpr int R = decltype(r_tag)::value;
+        constexpr int RS = phase_stride(R);
+        const int nup = sJ.S.up.count, ndn = sJ.S.dn.count, k = sS.k;
+        const double2* __restrict__ pin = sJ.YW[(k + 1) & 1];
+        double2* __restrict__ pout = sJ.YW[k & 1];
+        const double am = -sS.a_prev, bk = sS.b_cur, rb = 1.0 / bk, n0 = sS.norm0;
+        const bool first = (k == 1);
+        const bool coeff = (sJ.mode == LZ_COEFF);
+        const double ck = coeff ? 0.0 : sJ.coeff[k - 1];
+        const int r0 = tl * R, nr = min(R, ndn - r0);
+        double* xs = chunk;                              // [nup][RS] w_k
+        double* ps = chunk + nup * RS;                   // [nup][RS] w_{k-1}
+        // w at a global index, as its owner forms it (exchange terms)
+        auto fetch_w = [&](long long idx) {
+            EDZT_OK_OR(idx >= 0 && idx < sJ.S.dim, 21, idx, sJ.S.dim, k, return 0.0)
+            const double v = form_v(sJ, k, pin, am, idx);
+            return first ? v / n0 : v * rb;
+        };
+        for (int iu = threadIdx.x; iu < nup; iu += T) {
+            double w[R], wp[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                w[r] = wp[r] = 0.0;
+                if (r < nr) {
+                    const long long e = (long long)(r0 + r) * nup + iu;
+                    if (first) {
+                        w[r] = init_value(sJ, e) / n0;   // the reference divides (:130)
+                    } else {
+                        const double2 pr = __ldcg(pin + e);
+                        w[r] = fma(am, pr.y, pr.x) * rb;
+                        wp[r] = pr.y;
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                xs[iu * RS + r] = w[r];
+                ps[iu * RS + r] = wp[r];
+            }
+        }
+        double e1d[R];
+        int pd[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int id = min(r0 + r, ndn - 1);
+            e1d[r] = __ldg(sJ.S.dn.e1 + id);
+            pd[r] = __ldg(sJ.S.dn.imp + id);
+        }
+        __syncthreads();
+        for (int iu = threadIdx.x; iu < nup; iu += T) {
+            double hv[R];
+            row_part<R, RS>(sJ.S, xs, wint, amp_up, iu, e1d, pd, hv);
+            const int pu = sJ.S.has_j ? (int)__ldg(sJ.S.up.imp + iu) : 0;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                if (r >= nr) break;
+                const long long e = (long long)(r0 + r) * nup + iu;
+                const double dd = __ldcg(sJ.D + e);
+                double y = hv[r] + (first ? dd / n0 : dd * rb);
+                if (sJ.S.has_j) y = exchange_part(sJ.S, r0 + r, iu, pu, pd[r], y, fetch_w);
+                const double w = xs[iu * RS + r];
+                if (!first) y = fma(-bk, ps[iu * RS + r], y);
+                __stcg(pout + e, make_double2(y, w));
                 if (coeff) {
-                    const double t = fma(am, xe, y);         // y - a_{k-1} w (a_0 = 0)
-                    acc[0] = fma(xe, t, acc[0]);
-                    acc[1] = fma(t, t, acc[1]);
-                    acc[2] = fma(xe, xe, acc[2]);
+                    acc = fma(w, y, acc);
                 } else {
-                    __stcg(Et + e, FIRST ? ck * xe : fma(ck, xe, eprev));
+                    double* ep = sJ.eig + e;
+                    __stcg(ep, first ? ck * w : fma(ck, w, __ldcg(ep)));
                 }
             }
         }
         __syncthreads();
     };
 
-    for (int pass = 0; pass < B.max_passes; pass++) {
+    unsigned running = 1u;
+    int p = 0;
+    for (; p < B.max_phases; p++) {
+        const int ph = p & 1;
+        const long long* pre = prefix + (size_t)ph * (B.njobs + 1);
         int cur = -1;
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        for (long long t = blockIdx.x; t < B.total_tiles; t += G) {
-            if (cur < 0 || t >= __ldg(prefix + cur + 1)) {
-                if (cur >= 0 && sS.active) flush(pass, acc);
-                cur = find_job(prefix, B.njobs, t);
-                begin_job(cur, pass);
-                acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
+        double acc = 0.0;
+        for (long long t = blockIdx.x; t < B.total[ph]; t += G) {
+            if (cur < 0 || t >= __ldg(pre + cur + 1)) {
+                if (cur >= 0 && sS.active) flush(ph, acc);
+                cur = find_job(pre, B.njobs, t);
+                begin_job(cur, p, false);
+                acc = 0.0;
             }
             if (!sS.active) continue;
-            const int tl = (int)(t - sJ.tile0);
-            if (pass == 0) init_tile(tl, acc);
-            else if (sS.k == 1) step_tile(std::true_type{}, tl, acc);
-            else step_tile(std::false_type{}, tl, acc);
+            const int tl = (int)(t - sJ.ph[ph].tile0);
+            const int wdt = sJ.ph[ph].width;
+            if (ph == 0) {
+                switch (wdt) {
+                case 16: col_tile(std::integral_constant<int, 16>{}, tl, acc); break;
+                case 8: col_tile(std::integral_constant<int, 8>{}, tl, acc); break;
+                case 4: col_tile(std::integral_constant<int, 4>{}, tl, acc); break;
+                default: col_tile(std::integral_constant<int, 2>{}, tl, acc); break;
+                }
+            } else {
+                switch (wdt) {
+                case 8: row_tile(std::integral_constant<int, 8>{}, tl, acc); break;
+                case 4: row_tile(std::integral_constant<int, 4>{}, tl, acc); break;
+                case 2: row_tile(std::integral_constant<int, 2>{}, tl, acc); break;
+                default: row_tile(std::integral_constant<int, 1>{}, tl, acc); break;
+                }
+            }
         }
-        if (cur >= 0 && sS.active) flush(pass, acc);
-        unsigned running = 0u;
+        if (cur >= 0 && sS.active) flush(ph, acc);
         if (!grid_barrier(sw, status, nbar, running, B)) return;
         if (running == 0u) break;
+    }
+    if (B.slice && running != 0u && p == B.max_phases) {  // budget spent: open every run's next step
+        const long long* pre = prefix;
+        int cur = -1;
+        for (long long t = blockIdx.x; t < B.total[0]; t += G) {
+            if (cur < 0 || t >= __ldg(pre + cur + 1)) {
+                cur = find_job(pre, B.njobs, t);
+                begin_job(cur, p, true);
+            }
+        }
     }
 }
 
@@ -491,23 +469,97 @@ int lz_debug_bad(long long* out4)
 }
 #endif
 
-int lz_grid_size(int device, size_t smem, int* block_out)
+int lz_grid_size(int device, size_t smem, int block)
 {
     static std::atomic<unsigned long long> attr{0};
     if (edzt_once_per_device(attr))
-        cudaFuncSetAttribute(k_lanczos, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_lanczos, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLzSmemMax);
     int per_sm = 0, nsm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos, kLzThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos, block, smem);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    if (block_out) *block_out = kLzThreads;
     return per_sm * nsm;
 }
 
-cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, LzState* state, const long long* tile_prefix,
-                                      double* partials, unsigned* sync_words, int* status, cudaStream_t s)
+cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, const long long* prefix, double* slots,
+                                      unsigned* sync_words, int* status, cudaStream_t s)
 {
     LzBatch b = B;
-    void* args[] = {(void*)&b, (void*)&jobs, (void*)&state, (void*)&tile_prefix, (void*)&partials,
-                    (void*)&sync_words, (void*)&status};
+    void* args[] = {(void*)&b, (void*)&jobs, (void*)&prefix, (void*)&slots, (void*)&sync_words, (void*)&status};
     return cudaLaunchCooperativeKernel((const void*)k_lanczos, dim3(B.grid), dim3(B.block), args, B.smem, s);
+}
+
+// ---------------------------------------------------------------------------
+// launch plan
+// ---------------------------------------------------------------------------
+// Per-CTA dynamic shared memory: two CTAs of 256 threads per SM when every
+// job fits, else one CTA of 512 threads per SM.
+static constexpr size_t kLzSmemTwoPerSm = 108 * 1024;
+
+// Width (of opts, descending) for `count` lines, each tile needing need(w)
+// bytes of the budget: with few tiles in the launch, the one that minimises
+// the lines one CTA sweeps when the job runs alone, ceil(tiles / G) * w
+// (ties to the wider); with many, the widest that fits.
+template <class Need>
+static int pick_width(const int* opts, int nopt, int count, size_t budget, int G, bool many, Need need)
+{
+    int best = -1;
+    long long best_cost = -1;
+    for (int i = 0; i < nopt; i++) {
+        const int w = opts[i];
+        if (need(w) > budget) continue;
+        if (many) return w;
+        const long long tiles = (count + w - 1) / w;
+        const long long cost = ((tiles + G - 1) / G) * w;
+        if (best < 0 || cost < best_cost) { best = w; best_cost = cost; }
+    }
+    return best < 0 ? opts[nopt - 1] : best;
+}
+
+LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix)
+{
+    LzPlan P;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    const size_t fixed = lz_fixed_smem();
+    size_t need_min = 0;
+    long long lines8 = 0;
+    for (int j = 0; j < nj; j++) {
+        const int nup = jobs[j].S.up.count, ndn = jobs[j].S.dn.count;
+        need_min = std::max(need_min, std::max(lz_row_smem(nup, 1), lz_col_smem(ndn, 2)));
+        lines8 += (ndn + 7) / 8 + (nup + 15) / 16;
+    }
+    const bool two = fixed + need_min <= kLzSmemTwoPerSm;
+    P.block = two ? 256 : 512;
+    const size_t budget = (two ? kLzSmemTwoPerSm : kLzSmemMax) - fixed;
+    const int G_est = (two ? 2 : 1) * nsm;
+    const bool many = lines8 >= 4LL * G_est;
+    const int ropts[4] = {8, 4, 2, 1}, copts[4] = {16, 8, 4, 2};
+    size_t chunk = 0;
+    for (int j = 0; j < nj; j++) {
+        LzJob& J = jobs[j];
+        const int nup = J.S.up.count, ndn = J.S.dn.count;
+        J.ph[0].width = pick_width(copts, 4, nup, budget, G_est, many, [&](int w) { return lz_col_smem(ndn, w); });
+        J.ph[1].width = pick_width(ropts, 4, ndn, budget, G_est, many, [&](int w) { return lz_row_smem(nup, w); });
+        chunk = std::max(chunk, std::max(lz_col_smem(ndn, J.ph[0].width), lz_row_smem(nup, J.ph[1].width)));
+    }
+    P.smem = fixed + chunk;
+    P.grid = lz_grid_size(device, P.smem, P.block);
+    if (P.grid <= 0) return P;
+    const int G = P.grid;
+    prefix.assign(2 * (size_t)(nj + 1), 0);
+    for (int ph = 0; ph < 2; ph++) {
+        long long* pre = prefix.data() + (size_t)ph * (nj + 1);
+        for (int j = 0; j < nj; j++) {
+            LzPhase& Q = jobs[j].ph[ph];
+            const int count = (ph == 0) ? jobs[j].S.up.count : jobs[j].S.dn.count;
+            Q.ntiles = (count + Q.width - 1) / Q.width;
+            Q.tile0 = pre[j];
+            pre[j + 1] = pre[j] + Q.ntiles;
+            Q.npart = std::min(G, Q.ntiles);
+            Q.slot0 = P.slots;
+            P.slots += Q.npart;
+        }
+        P.total[ph] = pre[nj];
+    }
+    return P;
 }

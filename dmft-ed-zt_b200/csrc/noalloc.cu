@@ -8,7 +8,7 @@
 // call uses no device memory but the scratch array below and the context's
 // model tables, which an earlier allocating call on the same sector built.
 //
-// Scratch: one file-scope __device__ array of kNoAllocScratchBytes (8.2 MiB)
+// Scratch: one file-scope __device__ array of kNoAllocScratchBytes (10.1 MiB)
 // that every GPU which loads the library holds until the process exits.  It
 // limits the sector to EDZT_NOALLOC_MAX_DIM states and the run to
 // EDZT_NOALLOC_MAX_STEPS steps.  The first call on each device looks the
@@ -22,6 +22,7 @@
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
+#include <vector>
 #include <string>
 #include <cuda_runtime.h>
 #include "../../include/edzt.h"
@@ -38,14 +39,15 @@ constexpr size_t al(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 constexpr size_t kOffJob = 0;
 constexpr size_t kOffState = kOffJob + al(2048);        // LzJob
 constexpr size_t kOffPrefix = kOffState + al(2 * sizeof(LzState));
-constexpr size_t kOffStatus = kOffPrefix + al(2 * sizeof(long long));
+constexpr size_t kOffStatus = kOffPrefix + al(4 * sizeof(long long));
 constexpr size_t kOffSync = kOffStatus + al(sizeof(int));
 constexpr size_t kSyncBytes = al(sizeof(unsigned) * (128 + 32 * ((kMaxGrid + 15) / 16)));
-constexpr size_t kOffPart = kOffSync + kSyncBytes;      // [kMaxGrid][2][4] doubles
-constexpr size_t kOffAB = kOffPart + al(sizeof(double) * 8 * kMaxGrid);
+constexpr size_t kOffSlots = kOffSync + kSyncBytes;     // [2 phases * kMaxGrid][2] doubles
+constexpr size_t kOffAB = kOffSlots + al(sizeof(double) * 4 * kMaxGrid);
 constexpr size_t kOffYW = kOffAB + al(sizeof(double) * 2 * EDZT_NOALLOC_MAX_STEPS);
 constexpr size_t kYWBytes = sizeof(double2) * (size_t)EDZT_NOALLOC_MAX_DIM;
-constexpr size_t kNoAllocScratchBytes = kOffYW + 2 * kYWBytes;
+constexpr size_t kOffD = kOffYW + 2 * kYWBytes;
+constexpr size_t kNoAllocScratchBytes = kOffD + sizeof(double) * (size_t)EDZT_NOALLOC_MAX_DIM;
 
 static_assert(sizeof(LzJob) <= 2048, "job descriptor outgrew its scratch slot");
 
@@ -130,38 +132,32 @@ void run(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, 
     long long* d_prefix = reinterpret_cast<long long*>(base + kOffPrefix);
     int* d_status = reinterpret_cast<int*>(base + kOffStatus);
     unsigned* d_sync = reinterpret_cast<unsigned*>(base + kOffSync);
-    double* d_part = reinterpret_cast<double*>(base + kOffPart);
+    double* d_slots = reinterpret_cast<double*>(base + kOffSlots);
     double* d_a = reinterpret_cast<double*>(base + kOffAB);
     double* d_b = d_a + EDZT_NOALLOC_MAX_STEPS;
     double2* d_yw0 = reinterpret_cast<double2*>(base + kOffYW);
     double2* d_yw1 = reinterpret_cast<double2*>(base + kOffYW + kYWBytes);
+    double* d_d = reinterpret_cast<double*>(base + kOffD);
 
     LzJob J;
     std::memset(&J, 0, sizeof(J));
     J.S = S;
     J.YW[0] = d_yw0;
     J.YW[1] = d_yw1;
+    J.D = d_d;
     J.a = d_a;
     J.b = d_b;
     J.maxnstep = maxnstep;
     J.mode = LZ_COEFF;
     J.init = LZ_INIT_COPY;
-    J.rows = lz_rows_per_tile(S.up.count, S.dn.count, S.dn.hw);
-    J.ntiles = (S.dn.count + J.rows - 1) / J.rows;
-    const size_t smem = lz_smem_bytes(S.up.count, S.dn.hw, J.rows);
-    int block = 0;
-    int G = lz_grid_size(device, smem, &block);
-    if (G <= 0) throw Fail{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
-    if (G > kMaxGrid) G = kMaxGrid;
-    if (J.ntiles < 4 * G) {                              // spread a small sector over the grid, as the allocating path does
-        J.rows = lz_rows_balanced(S.dn.count, J.rows, G);
-        J.ntiles = (S.dn.count + J.rows - 1) / J.rows;
-    }
-    J.npart = J.ntiles < G ? J.ntiles : G;
-    J.tile0 = 0;
-    J.slot0 = 0;
-    // The start vector is read in the first pass only, which writes YW[1];
-    // a host vector is staged in YW[0], first overwritten by the second pass.
+    J.st = d_state;
+    // the same tile shapes, grid and shared memory as the allocating path
+    std::vector<long long> prefix;
+    const LzPlan P = lz_plan(device, &J, 1, prefix);
+    if (P.grid <= 0) throw Fail{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
+    if (P.grid > kMaxGrid) throw Fail{EDZT_ERR_CUDA, "persistent grid larger than the no-allocation sync area"};
+    // The start vector is read in the first step only (both phases), which
+    // writes YW[1]; a host vector is staged in YW[0], first written by step 2.
     if (is_device_ptr(v_init, device)) {
         J.src = v_init;
     } else {
@@ -170,28 +166,28 @@ void run(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, 
     }
     LzState hs[2];
     std::memset(hs, 0, sizeof(hs));
-    hs[0].active = 1;
-    const long long hprefix[2] = {0, J.ntiles};
+    hs[1].active = 1;                                    // the state before phase 0 (parity 1)
     // what must start at zero: the barrier's sync words (but the count of
     // runs still going, one), status, a, b
     const unsigned runs_going = 1u;
-    NA_CK(cudaMemsetAsync(d_sync, 0, lz_sync_bytes(G), st));
+    NA_CK(cudaMemsetAsync(d_sync, 0, lz_sync_bytes(P.grid), st));
     NA_CK(cudaMemcpyAsync(d_sync + 64, &runs_going, sizeof(unsigned), cudaMemcpyHostToDevice, st));
     NA_CK(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     NA_CK(cudaMemsetAsync(d_a, 0, sizeof(double) * 2 * EDZT_NOALLOC_MAX_STEPS, st));
     NA_CK(cudaMemcpyAsync(d_job, &J, sizeof(J), cudaMemcpyHostToDevice, st));
     NA_CK(cudaMemcpyAsync(d_state, hs, sizeof(hs), cudaMemcpyHostToDevice, st));
-    NA_CK(cudaMemcpyAsync(d_prefix, hprefix, sizeof(hprefix), cudaMemcpyHostToDevice, st));
+    NA_CK(cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(long long) * prefix.size(), cudaMemcpyHostToDevice, st));
     LzBatch B;
     std::memset(&B, 0, sizeof(B));
     B.njobs = 1;
-    B.grid = G;
-    B.block = block;
-    B.smem = smem;
-    B.total_tiles = J.ntiles;
-    B.max_passes = 2 * maxnstep + 4;
+    B.grid = P.grid;
+    B.block = P.block;
+    B.smem = P.smem;
+    B.total[0] = P.total[0];
+    B.total[1] = P.total[1];
+    B.max_phases = 2 * maxnstep + 4;
     B.stall_cta = -1;
-    NA_CK(launch_lanczos_persistent(B, d_job, d_state, d_prefix, d_part, d_sync, d_status, st));
+    NA_CK(launch_lanczos_persistent(B, d_job, d_prefix, d_slots, d_sync, d_status, st));
     edzt_count_launches(c, 1);
     int status = 0;
     NA_CK(cudaMemcpyAsync(hs, d_state, sizeof(hs), cudaMemcpyDeviceToHost, st));

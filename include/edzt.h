@@ -108,7 +108,7 @@ int edzt_lanczos_iteration(edzt_ctx *ctx, int ne_up, int ne_dn, const double *v_
  * owned entirely by another allocator, or a latency-critical loop that must
  * not take the device-wide synchronisation an allocation can cause.  Same
  * arguments and results as edzt_lanczos_iteration, always on the persistent
- * kernel, whose scratch is one static device array of about 8.2 MiB that
+ * kernel, whose scratch is one static device array of about 10.1 MiB that
  * every GPU loading the library holds until exit.  Limits: sector dimension
  * <= EDZT_NOALLOC_MAX_DIM, maxnstep <= EDZT_NOALLOC_MAX_STEPS (EDZT_ERR_ARG
  * beyond).  The sector's tables must already exist on the context (built by
@@ -235,23 +235,33 @@ int edzt_solve_batch(edzt_ctx *ctx, int ninst, const edzt_instance *inst, int ma
 
 /* Served form: continuous batching of impurity solves on one context.
  * Requests (edzt_instance, copied at submit) wait in a queue and are
- * admitted by their device-memory footprint (the sector scan's 32 B per
+ * admitted by their device-memory footprint (the sector scan's 40 B per
  * state, or the Green's runs') while the admitted ones fit hbm_budget (0: 80%
  * of the free memory; a request is always admitted when nothing else runs).
- * Every edzt_server_step runs one persistent launch carrying the current
- * phase of every admitted request -- sector scan, eigenvector pass, or c / c^+
- * runs plus continued fractions -- so each request finishes in three steps
- * and requests submitted meanwhile join at the next step.  A request's result
- * is the same as edzt_solve's on it alone, to rounding.  maxnstep, nw, omega
- * are fixed per server; destroy the server before its context. */
+ * A request goes through three phases -- sector scan, eigenvector pass, c / c^+
+ * runs plus continued fractions -- whose Lanczos runs live on the device
+ * across launches.  Requests fall in size classes (by nsite; up to nsite 11
+ * in one class).  Every edzt_server_step serves the next class in turn: it
+ * runs persistent launches of a budget of Lanczos phases over that class's
+ * runs (each launch ends with the unfinished runs' next step opened, and a
+ * later launch resumes them) and moves requests on as their phase's runs
+ * finish, until the step's time budget (edzt_server_set_step_ms, default 25
+ * ms) is spent or the class has nothing left to run.  Requests submitted
+ * meanwhile join at the next step.  A request's result is the same as
+ * edzt_solve's on it alone, to rounding.  maxnstep, nw, omega are fixed per
+ * server; destroy the server before its context. */
 typedef struct edzt_server edzt_server;
 int edzt_server_create(edzt_ctx *ctx, int maxnstep, int nw, const double *omega, size_t hbm_budget,
                        edzt_server **out);
 /* Queues one request; *id identifies it. */
 int edzt_server_submit(edzt_server *srv, const edzt_instance *inst, long long *id);
-/* Admits what fits and advances every admitted request by one phase (blocks
- * until the step's GPU work is done).  nactive, nqueued, nfinished nullable. */
+/* Admits what fits and serves the next size class for up to the step's time
+ * budget (blocks until the step's GPU work is done).  nactive, nqueued,
+ * nfinished nullable. */
 int edzt_server_step(edzt_server *srv, int *nactive, int *nqueued, int *nfinished);
+/* Time budget of one step in milliseconds (> 0; at least one launch of two
+ * Lanczos phases runs per step whatever the budget). */
+int edzt_server_set_step_ms(edzt_server *srv, double ms);
 /* *done = 1 and the results (isector, e0, G_cl(nw, norb, nspin) complex; all
  * nullable) once request id has finished, which also releases it; *done = 0
  * while it runs. */
@@ -263,8 +273,9 @@ int edzt_server_result(edzt_server *srv, long long id, int *done, int *isector, 
 int edzt_server_cancel(edzt_server *srv, long long id);
 void edzt_server_destroy(edzt_server *srv);
 /* Device-memory footprint (bytes) a request holds at its peak in the batched
- * and served forms: the sector scan's pair buffers (32 B per state of every
- * sector) or its Green's runs', whichever is larger, plus its ground state. */
+ * and served forms: the sector scan's pair and down-hop buffers (40 B per
+ * state of every sector) or its Green's runs', whichever is larger, plus its
+ * ground state. */
 int edzt_instance_footprint(const edzt_instance *inst, long long *bytes);
 
 /* Fault tests (no counterpart in the reference; no GPU fault is involved):

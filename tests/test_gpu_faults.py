@@ -74,6 +74,7 @@ def test_server_rejects_over_budget_and_cancels(pkg, solver, configs):
         ref.append(solver.solve(r["sectors"], 60, omega, nspin=1, seed=r["seed"]))
     sv = pkg.Server(solver, 60, omega, hbm_budget=int(2.5 * fp))                  # two run at a time
     try:
+        sv.set_step_ms(0.01)                                                        # one launch per step
         ids = [sv.submit(r) for r in reqs]
         sv.step()                                                                   # 0, 1 running; 2, 3 queued
         sv.cancel(ids[1])                                                           # a running request
@@ -81,7 +82,9 @@ def test_server_rejects_over_budget_and_cancels(pkg, solver, configs):
         with pytest.raises(pkg.EDError):
             sv.cancel(12345)
         res = {}
-        for _ in range(10):
+        for _ in range(5000):
+            if len(res) == 2:
+                break
             sv.step()
             for i in (0, 2):
                 if i not in res:

@@ -53,7 +53,7 @@ def test_server_mix_equals_alone(pkg, solver, configs):
         sv.step()
         ids.append(sv.submit(reqs[5]))
         res = {}
-        for _ in range(12):
+        for _ in range(2000):
             na, nq, nf = sv.step()
             for i, rid in enumerate(ids):
                 if i not in res:
@@ -79,11 +79,14 @@ def test_server_budget_admits_one_at_a_time(pkg, solver, configs):
     budget = int(1.5 * max(solver.footprint(r) for r in reqs))                      # one fits at a time
     sv = pkg.Server(solver, 80, omega, hbm_budget=budget)
     try:
+        sv.set_step_ms(0.01)                                # one launch of two phases per step
         ids = [sv.submit(r) for r in reqs]
         na, nq, nf = sv.step()
         assert na == 1 and nq == 2                          # the budget holds the others back
         res = {}
-        for _ in range(12):
+        for _ in range(5000):
+            if len(res) == len(reqs):
+                break
             sv.step()
             for i, rid in enumerate(ids):
                 if i not in res:
