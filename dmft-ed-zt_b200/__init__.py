@@ -51,7 +51,8 @@ EXPORTS = (
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
     "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
     "edzt_cluster_green_matrix", "edzt_gs_occupancy", "edzt_green_real", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
-    "edzt_server_cancel", "edzt_server_set_step_ms", "edzt_instance_footprint", "edzt_set_fault_test", "edzt_diag_arpack",
+    "edzt_server_cancel", "edzt_server_set_step_ms", "edzt_tune_sector", "edzt_clear_tuning",
+    "edzt_instance_footprint", "edzt_set_fault_test", "edzt_diag_arpack",
     "edzt_set_diag_solver", "edzt_hybridization", "edzt_local_green_bethe", "edzt_fit_bath", "edzt_dmft_bethe",
 )
 # ground_state's diag_solver values (src/ground_state.f90:53-60).
@@ -186,6 +187,8 @@ def load_library(path: str = LIB_PATH):
     L.edzt_server_destroy.restype = None
     L.edzt_server_cancel.argtypes = [_vp, C.c_longlong]
     L.edzt_server_set_step_ms.argtypes = [_vp, C.c_double]
+    L.edzt_tune_sector.argtypes = [_vp, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _dp]
+    L.edzt_clear_tuning.argtypes = [_vp]
     L.edzt_instance_footprint.argtypes = [_vp, C.POINTER(C.c_longlong)]
     L.edzt_set_fault_test.argtypes = [_vp, C.c_int, C.c_double, C.c_int]
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
@@ -535,6 +538,19 @@ class Solver:
         self._check(self._L.edzt_cluster_green_matrix(self._h, nspin, maxnstep, nw, _ptr(omega), _ptr(G)))
         Gc = (G[0::2] + 1j * G[1::2]).reshape(nspin, norb, norb, nw)   # [s, b, a, iw]
         return Gc.transpose(0, 2, 1, 3)
+
+    def tune_sector(self, ne_up, ne_dn, steps=12):
+        """Autotune the persistent kernel's tile shape for a sector shape
+        (edzt_tune_sector): returns dict(cols_per_slab, rows_per_tile, block,
+        ms_per_step) of the fastest shape, recorded on the context."""
+        wc, r, blk = C.c_int(), C.c_int(), C.c_int()
+        ms = C.c_double()
+        self._check(self._L.edzt_tune_sector(self._h, ne_up, ne_dn, steps, C.byref(wc), C.byref(r), C.byref(blk),
+                                             C.byref(ms)))
+        return dict(cols_per_slab=wc.value, rows_per_tile=r.value, block=blk.value, ms_per_step=ms.value)
+
+    def clear_tuning(self):
+        self._check(self._L.edzt_clear_tuning(self._h))
 
     def set_fault_test(self, pass_cap=0, wait_seconds=0.0, stall_cta=-1):
         """Fault tests of the persistent kernel (edzt_set_fault_test); all

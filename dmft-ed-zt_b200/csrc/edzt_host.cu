@@ -213,6 +213,9 @@ struct edzt_ctx {
     int dbg_pass_cap = 0;
     unsigned long long dbg_wait_ns = 0;
     int dbg_stall_cta = -1;
+    // tile shapes chosen by edzt_tune_sector, by (up strings, down strings)
+    struct Tuned { int wc, r, block; double ms_per_step; };
+    std::map<std::pair<int, int>, Tuned> tuned;
 };
 
 namespace {
@@ -486,7 +489,27 @@ struct JobSpec {
     double norm0 = 0.0;
 };
 
-void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
+// Widths preset on the jobs from the context's tuning table (the widest
+// tuned job decides the block size), or forced (force_* > 0, the tuner).
+int preset_widths(edzt_ctx* c, std::vector<LzJob>& jobs, int force_wc, int force_r, int force_block)
+{
+    if (force_block > 0) {
+        for (LzJob& J : jobs) { J.ph[0].width = force_wc; J.ph[1].width = force_r; }
+        return force_block;
+    }
+    int block = 0;
+    long long widest = -1;
+    for (LzJob& J : jobs) {
+        auto it = c->tuned.find({J.S.up.count, J.S.dn.count});
+        if (it == c->tuned.end()) continue;
+        J.ph[0].width = it->second.wc;
+        J.ph[1].width = it->second.r;
+        if (J.S.dim > widest) { widest = J.S.dim; block = it->second.block; }
+    }
+    return block;
+}
+
+void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs, int force_wc = 0, int force_r = 0, int force_block = 0)
 {
     const int nj = (int)specs.size();
     if (nj == 0) return;
@@ -524,10 +547,11 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
             CK(cudaMemsetAsync(s.b, 0, sizeof(double) * s.maxnstep, c->stream));
         }
     }
-    // rows per tile and columns per slab of every job, tile lists of both
-    // phases, grid and shared memory (lz_plan)
+    // rows per tile and columns per slab of every job (tuned, else by
+    // lz_plan's rule), tile lists of both phases, grid and shared memory
+    const int prefer = preset_widths(c, jobs, force_wc, force_r, force_block);
     std::vector<long long> prefix;
-    const LzPlan P = lz_plan(c->device, jobs.data(), nj, prefix);
+    const LzPlan P = lz_plan(c->device, jobs.data(), nj, prefix, prefer);
     if (P.grid <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
     const int G = P.grid;
     std::vector<LzState> st(2 * (size_t)nj);
@@ -595,6 +619,50 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs)
     c->st_launches += 1;
     c->st_ms += ms;
     c->st_bytes += bytes;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner: the tile shapes of the persistent kernel for one sector shape,
+// chosen by timing short runs of every shape that fits: columns per slab WC
+// (the column phase's stripe width), rows per tile R, and the CTA shape (two
+// CTAs of 256 threads per SM, or one of 512).  The best is recorded on the
+// context for the sector's (up strings, down strings) and used by every
+// later launch whose budget allows it.
+// ---------------------------------------------------------------------------
+edzt_ctx::Tuned tune_sector(edzt_ctx* c, int nu, int nd, int steps)
+{
+    const DevSector S = make_sector(c, nu, nd);
+    Lease<double> ab(c->pool, (size_t)2 * steps);
+    auto run = [&](int wc, int r, int block) {
+        std::vector<JobSpec> specs(1);
+        specs[0].nu = nu; specs[0].nd = nd;
+        specs[0].mode = LZ_COEFF;
+        specs[0].init = LZ_INIT_HASH;
+        specs[0].key = edzt_stream_key(0x7475e3ull, 0);
+        specs[0].maxnstep = steps;
+        specs[0].a = ab.p;
+        specs[0].b = ab.p + steps;
+        const double ms0 = c->st_ms;
+        run_jobs(c, specs, wc, r, block);
+        return (c->st_ms - ms0) / std::max(1, specs[0].nstep);
+    };
+    const size_t fixed = lz_fixed_smem();
+    edzt_ctx::Tuned best{0, 0, 0, HUGE_VAL};
+    run(2, 1, 512);                                       // warm-up
+    for (int block : {256, 512}) {
+        const size_t budget = (block == 256 ? 108 * 1024 : kLzSmemMax) - fixed;
+        for (int wc : {16, 8, 4, 2}) {
+            if (lz_col_smem(S.dn.count, wc) > budget) continue;
+            for (int r : {8, 4, 2, 1}) {
+                if (lz_row_smem(S.up.count, r) > budget) continue;
+                const double ms = run(wc, r, block);
+                if (ms < best.ms_per_step) best = {wc, r, block, ms};
+            }
+        }
+    }
+    if (best.wc == 0) throw EdztError{EDZT_ERR_ARG, "no tile shape of this sector fits shared memory"};
+    c->tuned[{S.up.count, S.dn.count}] = best;
+    return best;
 }
 
 // ---------------------------------------------------------------------------
@@ -1711,8 +1779,9 @@ float run_slice(edzt_ctx* c, std::vector<LiveJob*>& v, int phases)
         J.src = L.spec.ac_src;
         J.st = L.st.p;
     }
+    const int prefer = preset_widths(c, jobs, 0, 0, 0);
     std::vector<long long> prefix;
-    const LzPlan P = lz_plan(c->device, jobs.data(), nj, prefix);
+    const LzPlan P = lz_plan(c->device, jobs.data(), nj, prefix, prefer);
     if (P.grid <= 0) throw EdztError{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t bytes_jobs = sizeof(LzJob) * nj, bytes_pre = sizeof(long long) * prefix.size();
@@ -2485,6 +2554,27 @@ int edzt_server_step(edzt_server* sv, int* nactive, int* nqueued, int* nfinished
         if (nactive) *nactive = (int)sv->active.size();
         if (nqueued) *nqueued = (int)sv->queue.size();
     });
+}
+
+int edzt_tune_sector(edzt_ctx* c, int ne_up, int ne_dn, int steps, int* wc, int* rows, int* block,
+                     double* ms_per_step)
+{
+    return guarded(c, [&] {
+        require_model(c);
+        check_sector(c, ne_up, ne_dn);
+        arg_check(steps >= 2 && steps <= 1000, "steps in [2, 1000]");
+        arg_check(sector_dim(c, ne_up, ne_dn) > 0, "empty sector");
+        const edzt_ctx::Tuned t = tune_sector(c, ne_up, ne_dn, steps);
+        if (wc) *wc = t.wc;
+        if (rows) *rows = t.r;
+        if (block) *block = t.block;
+        if (ms_per_step) *ms_per_step = t.ms_per_step;
+    });
+}
+
+int edzt_clear_tuning(edzt_ctx* c)
+{
+    return guarded(c, [&] { c->tuned.clear(); });
 }
 
 int edzt_server_set_step_ms(edzt_server* sv, double ms)

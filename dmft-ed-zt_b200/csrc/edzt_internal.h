@@ -176,8 +176,10 @@ size_t lz_fixed_smem();
 // Sync-word buffer size (bytes) for a grid of G CTAs.
 size_t lz_sync_bytes(int G);
 // Tile shapes of the jobs of one launch: every job's rows per tile and
-// columns per slab, the launch's block size, grid and shared memory; the
-// phases' tile lists, participants and slots are filled in.
+// columns per slab (a nonzero jobs[j].ph[].width on entry is a preset, kept
+// when it fits), the launch's block size (prefer_block 512: one CTA of 512
+// threads per SM even when two of 256 would fit), grid and shared memory;
+// the phases' tile lists, participants and slots are filled in.
 struct LzPlan {
     int block = 256;
     int grid = 0;
@@ -185,7 +187,7 @@ struct LzPlan {
     long long total[2] = {0, 0};
     long long slots = 0;
 };
-LzPlan lz_plan(int device, LzJob* jobs, int njobs, std::vector<long long>& prefix);
+LzPlan lz_plan(int device, LzJob* jobs, int njobs, std::vector<long long>& prefix, int prefer_block = 0);
 
 // ---- edzt_host.cu: context accessors (no table building, no allocation) -----
 struct edzt_ctx;

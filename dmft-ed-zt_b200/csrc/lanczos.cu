@@ -515,7 +515,7 @@ static int pick_width(const int* opts, int nopt, int count, size_t budget, int G
     return best < 0 ? opts[nopt - 1] : best;
 }
 
-LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix)
+LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, int prefer_block)
 {
     LzPlan P;
     int nsm = 148;
@@ -528,7 +528,7 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix)
         need_min = std::max(need_min, std::max(lz_row_smem(nup, 1), lz_col_smem(ndn, 2)));
         lines8 += (ndn + 7) / 8 + (nup + 15) / 16;
     }
-    const bool two = fixed + need_min <= kLzSmemTwoPerSm;
+    const bool two = fixed + need_min <= kLzSmemTwoPerSm && prefer_block != 512;
     P.block = two ? 256 : 512;
     const size_t budget = (two ? kLzSmemTwoPerSm : kLzSmemMax) - fixed;
     const int G_est = (two ? 2 : 1) * nsm;
@@ -538,8 +538,12 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix)
     for (int j = 0; j < nj; j++) {
         LzJob& J = jobs[j];
         const int nup = J.S.up.count, ndn = J.S.dn.count;
-        J.ph[0].width = pick_width(copts, 4, nup, budget, G_est, many, [&](int w) { return lz_col_smem(ndn, w); });
-        J.ph[1].width = pick_width(ropts, 4, ndn, budget, G_est, many, [&](int w) { return lz_row_smem(nup, w); });
+        // a width preset by the tuner is kept when it fits this launch's budget
+        const int wc = J.ph[0].width, r = J.ph[1].width;
+        J.ph[0].width = (wc > 0 && lz_col_smem(ndn, wc) <= budget)
+                            ? wc : pick_width(copts, 4, nup, budget, G_est, many, [&](int w) { return lz_col_smem(ndn, w); });
+        J.ph[1].width = (r > 0 && lz_row_smem(nup, r) <= budget)
+                            ? r : pick_width(ropts, 4, ndn, budget, G_est, many, [&](int w) { return lz_row_smem(nup, w); });
         chunk = std::max(chunk, std::max(lz_col_smem(ndn, J.ph[0].width), lz_row_smem(nup, J.ph[1].width)));
     }
     P.smem = fixed + chunk;

@@ -278,6 +278,20 @@ void edzt_server_destroy(edzt_server *srv);
  * ground state. */
 int edzt_instance_footprint(const edzt_instance *inst, long long *bytes);
 
+/* Autotuner (north_star's tuned stripe width; no counterpart in the
+ * reference): times short Lanczos runs (`steps` steps, 2..1000) of the
+ * context's model on sector (ne_up, ne_dn) for every tile shape of the
+ * persistent kernel that fits -- columns per slab of the column phase (the
+ * stripe width: 2, 4, 8 or 16), rows per tile of the row phase (1, 2, 4 or
+ * 8), one CTA of 512 or two of 256 threads per SM -- and records the fastest
+ * on the context for that sector shape; later launches on the context use it
+ * for every run of that shape (results unchanged but for rounding).
+ * Outputs (nullable): the chosen shape and its time per Lanczos step.
+ * edzt_clear_tuning forgets every recorded shape. */
+int edzt_tune_sector(edzt_ctx *ctx, int ne_up, int ne_dn, int steps, int *cols_per_slab, int *rows_per_tile,
+                     int *block, double *ms_per_step);
+int edzt_clear_tuning(edzt_ctx *ctx);
+
 /* Fault tests (no counterpart in the reference; no GPU fault is involved):
  * pass_cap > 0 caps the passes of a persistent launch (a run that needs more
  * fails with EDZT_ERR_NUMERIC); wait_seconds > 0 shortens the grid-barrier
