@@ -637,6 +637,22 @@ def run_gpu(args):
                         "ground-state batch (9 sectors, 245 MB of vectors) exceeds L2, the eigenvector "
                         "and Green's-function launches (<= 27 MB) are L2-resident"}
     roofline["traffic"] = read_traffic(args.traffic_file)
+    # the launches of one solve separately: ground-state scan, eigenvector
+    # pass, c/c^+ runs (each timed solve makes these three, in this order)
+    log = s.launch_log()
+    names = ["ground-state scan (9 sectors, 300 steps)", "eigenvector pass (winning sector)",
+             "c / c^+ runs (2 excitation sectors, 300 steps)"]
+    if log and len(log) % 3 == 0:
+        per = []
+        for q in range(3):
+            ent = log[q::3]
+            ms = sum(e["ms"] for e in ent) / len(ent)
+            by = sum(e["bytes"] for e in ent) / len(ent)
+            gbs = by / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+            per.append({"launch": names[q], "avg_ms": ms, "algorithmic_bytes": by, "achieved_GBs": gbs,
+                        "frac": gbs / peak if peak else None, "states": ent[0]["states"],
+                        "pair_and_D_bytes": 40.0 * ent[0]["states"]})
+        roofline["per_launch"] = per
 
     hv = hv_leg(pkg, s, peak) if (world == 1 and not args.skip_hv) else None
     batched = served = None

@@ -49,7 +49,7 @@ EXPORTS = (
     "edzt_set_engine", "edzt_basis", "edzt_basis_rank", "edzt_sector_dim", "edzt_hx", "edzt_apply_c",
     "edzt_lanczos_iteration", "edzt_diag_lanczos", "edzt_ground_state", "edzt_gs_dim",
     "edzt_green_diag", "edzt_cluster_green_ftn", "edzt_solve", "edzt_launch_count", "edzt_get_stream",
-    "edzt_kernel_stats", "edzt_reset_stats", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
+    "edzt_kernel_stats", "edzt_reset_stats", "edzt_kernel_launch_log", "edzt_lanczos_iteration_noalloc", "edzt_solve_batch",
     "edzt_cluster_green_matrix", "edzt_gs_occupancy", "edzt_green_real", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
     "edzt_server_cancel", "edzt_server_set_step_ms", "edzt_tune_sector", "edzt_clear_tuning",
     "edzt_instance_footprint", "edzt_set_fault_test", "edzt_diag_arpack",
@@ -209,6 +209,7 @@ def load_library(path: str = LIB_PATH):
     L.edzt_get_stream.argtypes = [_vp, C.POINTER(C.c_void_p)]
     L.edzt_kernel_stats.argtypes = [_vp, C.POINTER(C.c_longlong), _dp, _dp]
     L.edzt_reset_stats.argtypes = [_vp]
+    L.edzt_kernel_launch_log.argtypes = [_vp, C.c_int, _ip, _vp, _vp, _vp]
     _lib = L
     return L
 
@@ -363,6 +364,13 @@ class Solver:
 
     def reset_stats(self):
         self._check(self._L.edzt_reset_stats(self._h))
+
+    def launch_log(self) -> list:
+        """Per persistent launch since the last reset: dict(ms, bytes, states)."""
+        ms, by, st = np.zeros(256), np.zeros(256), np.zeros(256)
+        n = C.c_int()
+        self._check(self._L.edzt_kernel_launch_log(self._h, 256, C.byref(n), _ptr(ms), _ptr(by), _ptr(st)))
+        return [dict(ms=float(ms[i]), bytes=float(by[i]), states=float(st[i])) for i in range(n.value)]
 
     def set_model(self, m: Model):
         em, ek, vmk = m.fortran_arrays()

@@ -216,6 +216,9 @@ struct edzt_ctx {
     // tile shapes chosen by edzt_tune_sector, by (up strings, down strings)
     struct Tuned { int wc, r, block; double ms_per_step; };
     std::map<std::pair<int, int>, Tuned> tuned;
+    // per launch since the last statistics reset: device ms, algorithmic
+    // bytes, states in the launch (the last kLaunchLog)
+    std::vector<double> log_ms, log_bytes, log_states;
 };
 
 namespace {
@@ -509,6 +512,16 @@ int preset_widths(edzt_ctx* c, std::vector<LzJob>& jobs, int force_wc, int force
     return block;
 }
 
+constexpr size_t kLaunchLog = 256;
+
+void log_launch(edzt_ctx* c, double ms, double bytes, double states)
+{
+    if (c->log_ms.size() >= kLaunchLog) return;
+    c->log_ms.push_back(ms);
+    c->log_bytes.push_back(bytes);
+    c->log_states.push_back(states);
+}
+
 void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs, int force_wc = 0, int force_r = 0, int force_block = 0)
 {
     const int nj = (int)specs.size();
@@ -619,6 +632,9 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs, int force_wc = 0, int fo
     c->st_launches += 1;
     c->st_ms += ms;
     c->st_bytes += bytes;
+    double states = 0.0;
+    for (int j = 0; j < nj; j++) states += (double)jobs[j].S.dim;
+    log_launch(c, ms, bytes, states);
 }
 
 // ---------------------------------------------------------------------------
@@ -1845,6 +1861,9 @@ float run_slice(edzt_ctx* c, std::vector<LiveJob*>& v, int phases)
     c->st_launches += 1;
     c->st_ms += ms;
     c->st_bytes += bytes;
+    double states = 0.0;
+    for (int j = 0; j < nj; j++) states += (double)jobs[j].S.dim;
+    log_launch(c, ms, bytes, states);
     return ms;
 }
 
@@ -2236,6 +2255,22 @@ int edzt_reset_stats(edzt_ctx* c)
     c->st_launches = 0;
     c->st_ms = 0.0;
     c->st_bytes = 0.0;
+    c->log_ms.clear();
+    c->log_bytes.clear();
+    c->log_states.clear();
+    return EDZT_OK;
+}
+
+int edzt_kernel_launch_log(edzt_ctx* c, int max, int* n, double* ms, double* bytes, double* states)
+{
+    if (!c || !n || max < 0) return EDZT_ERR_ARG;
+    const int k = (int)std::min<size_t>((size_t)max, c->log_ms.size());
+    for (int i = 0; i < k; i++) {
+        if (ms) ms[i] = c->log_ms[i];
+        if (bytes) bytes[i] = c->log_bytes[i];
+        if (states) states[i] = c->log_states[i];
+    }
+    *n = k;
     return EDZT_OK;
 }
 

@@ -369,6 +369,11 @@ int edzt_get_stream(edzt_ctx *ctx, void **stream);
  * c/c^+-projected one). */
 int edzt_kernel_stats(edzt_ctx *ctx, long long *launches, double *ms, double *bytes);
 int edzt_reset_stats(edzt_ctx *ctx);
+/* The same per launch, in launch order since the last reset (at most the
+ * first 256 launches): device ms, algorithmic bytes and the states (sum of
+ * the runs' sector dimensions) of each; *n receives the count returned (at
+ * most max).  ms, bytes, states nullable. */
+int edzt_kernel_launch_log(edzt_ctx *ctx, int max, int *n, double *ms, double *bytes, double *states);
 
 #ifdef __cplusplus
 }
