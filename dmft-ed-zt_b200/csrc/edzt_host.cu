@@ -542,7 +542,7 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs, int force_wc = 0, int fo
             bufs.emplace_back(c->pool, (size_t)dim);
             J.YW[q] = bufs.back().p;
         }
-        dbufs.emplace_back(c->pool, (size_t)dim);
+        dbufs.emplace_back(c->pool, (size_t)lz_d_size(J.S.up.count, J.S.dn.count));
         J.D = dbufs.back().p;
         J.eig = s.eig;
         J.coeff = s.coeff;
@@ -667,9 +667,9 @@ edzt_ctx::Tuned tune_sector(edzt_ctx* c, int nu, int nd, int steps)
     run(2, 1, 512);                                       // warm-up
     for (int block : {256, 512}) {
         const size_t budget = (block == 256 ? 108 * 1024 : kLzSmemMax) - fixed;
-        for (int wc : {16, 8, 4, 2}) {
+        for (int wc : {8, 4, 2}) {
             if (lz_col_smem(S.dn.count, wc) > budget) continue;
-            for (int r : {8, 4, 2, 1}) {
+            for (int r : {4, 2, 1}) {
                 if (lz_row_smem(S.up.count, r) > budget) continue;
                 const double ms = run(wc, r, block);
                 if (ms < best.ms_per_step) best = {wc, r, block, ms};
@@ -699,7 +699,8 @@ int plain_lanczos(edzt_ctx* c, const DevSector& S, const double* v_init, int max
                   double* norm_out, const double* coeff, double* eig)
 {
     const long long n = S.dim;
-    Lease<double> v(c->pool, (size_t)n), w(c->pool, (size_t)n), hs(c->pool, (size_t)n);
+    Lease<double> v(c->pool, (size_t)n), w(c->pool, (size_t)n),
+        hs(c->pool, (size_t)hx_scratch_size(S.up.count, S.dn.count));
     if (coeff == nullptr)
         for (int i = 0; i < maxnstep; i++) { a[i] = 0.0; b[i] = 0.0; }
     const double norm_v = std::sqrt(plain_dot(c, v_init, v_init, n));          // :128
@@ -764,7 +765,7 @@ double finish_eigvec(edzt_ctx* c, const DevSector& S, double* vec, double e0)
     double* sc = c->scal->as<double>();
     launch_dot(vec, vec, n, c->dot_part->as<double>(), sc, c->stream);
     launch_scale_inv_sqrt(vec, n, sc, c->stream);                              // :291
-    Lease<double> v(c->pool, (size_t)n), hs(c->pool, (size_t)n);
+    Lease<double> v(c->pool, (size_t)n), hs(c->pool, (size_t)hx_scratch_size(S.up.count, S.dn.count));
     launch_hx(S, vec, v.p, 0, hs.p, c->stream);
     launch_axpy(v.p, vec, n, nullptr, e0, -1.0, c->stream);
     c->launches += 7;
@@ -808,7 +809,7 @@ void diag_arpack_impl(edzt_ctx* c, const DevSector& S, uint64_t key, double* vec
     const int m = kArNcv, kmax = kArNev + (kArNcv - kArNev) / 2;
     const double eps = 0x1p-53, eps23 = std::pow(eps, 2.0 / 3.0), tol = eps;
     cudaStream_t st = c->stream;
-    Lease<double> buf(c->pool, (size_t)(m + 1 + kmax) * n), hxs(c->pool, (size_t)n);
+    Lease<double> buf(c->pool, (size_t)(m + 1 + kmax) * n), hxs(c->pool, (size_t)hx_scratch_size(S.up.count, S.dn.count));
     Lease<double> small(c->pool, (size_t)rl_partials_size() + 32 + EDZT_RL_MAXV * EDZT_RL_MAXV);
     double* part = small.p;
     double* hd = small.p + rl_partials_size();          // [0, 8) pass 1, [8, 16) pass 2, [16] |w|^2
@@ -1639,13 +1640,13 @@ void init_inst(const edzt_instance& in, BatchInst& I)
         const int nu = I.sec[2 * s], nd = I.sec[2 * s + 1];
         arg_check(sector_valid_ns(ns, nu, nd), "electron counts outside [0, nsite]");
         const long long d = sector_dim_ns(ns, nu, nd);
-        gsb += 40 * d;                                   // two pair buffers and D per run
+        gsb += 40 * d + 56 * sector_dim_ns(ns, 0, nd);   // two pair buffers and D (slab padding) per run
         maxd = std::max(maxd, d);
         for (int du = -1; du <= 1; du++)
             for (int dd = -1; dd <= 1; dd++)
                 if ((du == 0) != (dd == 0)) maxe = std::max(maxe, sector_dim_ns(ns, nu + du, nd + dd));
     }
-    const long long cfb = 4LL * I.model.norb * 40 * maxe + 8 * maxd;
+    const long long cfb = 4LL * I.model.norb * (40 * maxe + 56 * sector_dim_ns(ns, 0, ns / 2)) + 8 * maxd;
     I.footprint = std::max(gsb, cfb) + 56 * maxd;
 }
 
@@ -1754,7 +1755,7 @@ std::unique_ptr<LiveJob> make_live(edzt_ctx* c, const JobSpec& spec)
     L->S = make_sector_mt(c, spec.mt ? *spec.mt : c->mt, spec.nu, spec.nd);
     L->yw0 = Lease<double2>(c->pool, (size_t)L->S.dim);
     L->yw1 = Lease<double2>(c->pool, (size_t)L->S.dim);
-    L->d = Lease<double>(c->pool, (size_t)L->S.dim);
+    L->d = Lease<double>(c->pool, (size_t)lz_d_size(L->S.up.count, L->S.dn.count));
     L->st = Lease<LzState>(c->pool, 2);
     LzState init[2];
     std::memset(init, 0, sizeof(init));
@@ -2334,7 +2335,7 @@ int edzt_hx(edzt_ctx* c, int ne_up, int ne_dn, const double* x, double* y, int a
         InVec xi(c, x, S.dim);
         OutVec yo(c, y, S.dim);
         if (accumulate) yo.preload();
-        Lease<double> hs(c->pool, (size_t)std::max(S.dim, 1LL));
+        Lease<double> hs(c->pool, (size_t)std::max(hx_scratch_size(S.up.count, S.dn.count), 1LL));
         launch_hx(S, xi.d, yo.d, accumulate ? 1 : 0, hs.p, c->stream);
         c->launches += 2;
         CKLAUNCH();

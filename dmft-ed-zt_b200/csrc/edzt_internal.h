@@ -44,8 +44,10 @@ void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32
 int edzt_max_hops(const DevModel& m, int sigma, int n);
 
 // ---- kernels.cu: standalone (non-persistent) kernels ------------------------
-// H.v in two phases (hv_phase.cuh); scratch: dim doubles of device memory.
+// H.v in two phases (hv_phase.cuh); scratch: hx_scratch_size doubles of
+// device memory (the down-hop part, slab-major, slabs of up to 16 columns).
 void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, double* scratch, cudaStream_t s);
+inline long long hx_scratch_size(int nup, int ndn) { return (long long)((nup + 15) / 16) * 16 * ndn; }
 // Whether a sector's staged row and column slab fit in shared memory.
 bool hx_fits(int nup, int ndn);
 // Deterministic dot product: result written to *out (device).  partials needs
@@ -104,12 +106,12 @@ enum LzInit { LZ_INIT_HASH = 0, LZ_INIT_APPLYC = 1, LZ_INIT_COPY = 2 };
 // (tile0 + q) mod G, q < npart, and participant q owns partial-sum slot
 // slot0 + q.
 struct LzPhase {
-    long long tile0;
-    long long slot0;
+    long long tile0;      // first tile in the launch's tile list of the phase
+    long long slot0;      // first partial-sum slot
     int ntiles;
-    int npart;
+    int npart;            // participating CTAs: part0, part0 + 1, ..., one slot each
     int width;            // columns per slab (column phase) or rows per tile (row phase)
-    int pad;
+    int part0;
 };
 
 // Recurrence state of one run between phases (every participating CTA
@@ -130,7 +132,8 @@ struct LzState {
 struct LzJob {
     DevSector S;
     double2* YW[2];       // ping-pong pair buffers [dim]
-    double* D;            // [dim] down-hop part of H v_k, column phase -> row phase
+    double* D;            // [lz_d_size] down-hop part of H v_k, column phase -> row phase, slab-major:
+                          // the slab of columns [c0, c0 + WC) is the block [ndn][WC] at c0 * ndn
     double* eig;          // EIGVEC: output eigenvector (unnormalised)
     const double* coeff;  // EIGVEC: ground eigenvector of the tridiagonal [nstep]
     double* a;            // [maxnstep] a(1..), written as steps are accepted
@@ -145,6 +148,9 @@ struct LzJob {
     ApplyCArgs ac;        // LZ_INIT_APPLYC
     const double* src;    // LZ_INIT_APPLYC: the ground state; LZ_INIT_COPY: the start vector
 };
+
+// Doubles of a job's D buffer (slabs of up to 8 columns).
+inline long long lz_d_size(int nup, int ndn) { return (long long)((nup + 7) / 8) * 8 * ndn; }
 
 struct LzBatch {
     int njobs;
@@ -179,7 +185,11 @@ size_t lz_sync_bytes(int G);
 // columns per slab (a nonzero jobs[j].ph[].width on entry is a preset, kept
 // when it fits), the launch's block size (prefer_block 512: one CTA of 512
 // threads per SM even when two of 256 would fit), grid and shared memory;
-// the phases' tile lists, participants and slots are filled in.
+// the phases' tile lists, participants and slots are filled in.  prefix
+// receives, per phase, the jobs' first tiles [njobs + 1], then per phase
+// every CTA's first tile [grid + 1] (CTA b takes the contiguous tiles
+// [range[b], range[b + 1]), cut by tile cost so the CTAs finish together),
+// then the slab of each column-phase tile position [total[0]].
 struct LzPlan {
     int block = 256;
     int grid = 0;

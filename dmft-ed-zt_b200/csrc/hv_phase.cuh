@@ -34,17 +34,23 @@
 // (n = 1 stays 1: a single value, loaded as a scalar).
 __host__ __device__ constexpr int phase_stride(int n) { return n <= 1 ? 1 : ((n + 1) / 4) * 4 + 2; }
 
-// Hop entry h of string t in a packed table [hw/4][count] of uint4
-__device__ __forceinline__ uint32_t hop_entry(const DevSpin& sp, int t, int h)
-{
-    const uint32_t* hp = reinterpret_cast<const uint32_t*>(sp.hpk);
-    return __ldg(hp + ((size_t)(h >> 2) * sp.count + t) * 4 + (h & 3));
-}
-
 __device__ __forceinline__ void stage_table(const double* __restrict__ src, int n, double* dst)
 {
     for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
 }
+
+// Asynchronous 8-byte copy global -> shared (cp.async, no register holds the
+// value in flight, so a thread can have its whole share of a tile in flight
+// at once); when `valid` is false nothing is read and the destination gets 0.
+__device__ __forceinline__ void copy_async8(double* dst, const double* src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int bytes = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+
+// Wait for every asynchronous copy this thread issued (the caller then syncs the CTA).
+__device__ __forceinline__ void copy_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // acc[q] += a * line[q] for q < N, two at a time (16-byte shared loads).
 template <int N>
@@ -62,43 +68,129 @@ __device__ __forceinline__ void axpy_line(double a, const double* __restrict__ l
     }
 }
 
+// The packed hop list of string t (table [hw/4][count] of uint4): its count
+// and first eight entries, loaded as one byte and two 16-byte words.  A
+// loop over strings loads the next string's list before it uses the current
+// one, so the table's latency overlaps the current string's arithmetic.
+struct HopList {
+    int hc;
+    uint4 q0, q1;
+};
+
+__device__ __forceinline__ HopList hop_list(const DevSpin& sp, int t)
+{
+    HopList L;
+    const uint4* __restrict__ hp = sp.hpk + t;
+    L.hc = __ldg(sp.hcnt + t);
+    L.q0 = (sp.hw > 0) ? __ldg(hp) : make_uint4(0u, 0u, 0u, 0u);
+    L.q1 = (sp.hw > 4) ? __ldg(hp + sp.count) : make_uint4(0u, 0u, 0u, 0u);
+    return L;
+}
+
+// Hop sum of string t over staged lines: acc[q] += amp(h) * lines[rank(h) *
+// STRIDE + q] over the string's hops h, in table order.  The eight terms of
+// the loaded entries are issued without waiting on one another (lanes past
+// their string's hop count are predicated off); longer lists continue four
+// at a time.
+template <int N, int STRIDE>
+__device__ __forceinline__ void hop_sum(const DevSpin& sp, int t, const HopList& L, const double* __restrict__ amp,
+                                        const double* __restrict__ lines, double (&acc)[N], int code)
+{
+    const int hc = L.hc;
+    const uint32_t e[8] = {L.q0.x, L.q0.y, L.q0.z, L.q0.w, L.q1.x, L.q1.y, L.q1.z, L.q1.w};
+#pragma unroll
+    for (int h = 0; h < 8; h++) {
+        if (h < hc) {
+            EDZT_OK_OR(edzt_hop_rank(e[h]) < sp.count && edzt_hop_slot(e[h]) < sp.namp, code, t, h, (long long)e[h],
+                       continue)
+            axpy_line<N>(amp[edzt_hop_slot(e[h])], lines + edzt_hop_rank(e[h]) * STRIDE, acc);
+        }
+    }
+    for (int h0 = 8; h0 < hc; h0 += 4) {
+        const uint4 q = __ldg(sp.hpk + t + (size_t)(h0 >> 2) * sp.count);
+        const uint32_t f[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+            if (h0 + h < hc) {
+                EDZT_OK_OR(edzt_hop_rank(f[h]) < sp.count && edzt_hop_slot(f[h]) < sp.namp, code, t, h0 + h,
+                           (long long)f[h], continue)
+                axpy_line<N>(amp[edzt_hop_slot(f[h])], lines + edzt_hop_rank(f[h]) * STRIDE, acc);
+            }
+        }
+    }
+}
+
+// The down-hop part D written by the column phase is slab-major: the slab
+// of columns [c0, c0 + WC) is one contiguous block [ndn][WC] at c0 * ndn, so
+// a CTA writes its slab as one stream of 16-byte stores.  Element (id, iu)
+// with WC = 2^wsh:
+__device__ __forceinline__ long long slab_index(int id, int iu, int ndn, int wsh)
+{
+    return ((long long)(iu >> wsh) * ndn + id) * (1 << wsh) + (iu & ((1 << wsh) - 1));
+}
+
+// Store the WC values of row id of the slab starting at column c0 (16-byte
+// stores; c0 and WC are even, so every pair is 16-byte aligned).
+template <int WC>
+__device__ __forceinline__ void store_slab_row(double* __restrict__ D, int c0, int ndn, int id, const double (&d)[WC])
+{
+    double2* out = reinterpret_cast<double2*>(D + (long long)c0 * ndn + (long long)id * WC);
+#pragma unroll
+    for (int c = 0; c < WC; c += 2) __stcg(out + c / 2, make_double2(d[c], d[c + 1]));
+}
+
+// What the row phase reads from global memory for column iu of a tile of R
+// rows: the column's up string (energy, impurity bits, hop list) and the
+// down-hop part D of its R elements (slabs of 2^wsh columns); loaded one
+// column ahead.
+template <int R>
+struct RowCol {
+    double e1u;
+    int pu;
+    HopList L;
+    double dd[R];
+};
+
+template <int R>
+__device__ __forceinline__ RowCol<R> row_col(const DevSector& S, const double* __restrict__ D, int wsh, int iu,
+                                             int r0, int nr)
+{
+    RowCol<R> c;
+    c.e1u = __ldg(S.up.e1 + iu);
+    c.pu = __ldg(S.up.imp + iu);
+    c.L = hop_list(S.up, iu);
+#pragma unroll
+    for (int r = 0; r < R; r++) c.dd[r] = (r < nr) ? __ldcg(D + slab_index(r0 + r, iu, S.dn.count, wsh)) : 0.0;
+    return c;
+}
+
 // Row phase, column iu of a tile of R staged rows: the diagonal and up-hop
 // part of (H x)(r0 + r, iu) into acc[r].  xs: [nup][RS] staged values,
 // wint: [P*P], amp: up-hop amplitudes by slot, e1d/pd: the rows' down-string
-// energies and impurity patterns.
+// energies and impurity patterns, c: the column's prefetched data.
 template <int R, int RS>
 __device__ __forceinline__ void row_part(const DevSector& S, const double* __restrict__ xs,
                                          const double* __restrict__ wint, const double* __restrict__ amp, int iu,
-                                         const double (&e1d)[R], const int (&pd)[R], double (&acc)[R])
+                                         const RowCol<R>& c, const double (&e1d)[R], const int (&pd)[R],
+                                         double (&acc)[R])
 {
     const double* __restrict__ own = xs + iu * RS;
-    const double e1u = __ldg(S.up.e1 + iu);
-    const int pu = __ldg(S.up.imp + iu) * S.P;
+    const int pu = c.pu * S.P;
 #pragma unroll
-    for (int r = 0; r < R; r++) acc[r] = (e1u + e1d[r] + wint[pu + pd[r]]) * own[r];
-    const int hu = __ldg(S.up.hcnt + iu);
-    for (int h = 0; h < hu; h++) {
-        const uint32_t e = hop_entry(S.up, iu, h);
-        EDZT_OK_OR(edzt_hop_rank(e) < S.up.count && edzt_hop_slot(e) < S.up.namp, 71, iu, h, (long long)e, continue)
-        axpy_line<R>(amp[edzt_hop_slot(e)], xs + edzt_hop_rank(e) * RS, acc);
-    }
+    for (int r = 0; r < R; r++) acc[r] = (c.e1u + e1d[r] + wint[pu + pd[r]]) * own[r];
+    hop_sum<R, RS>(S.up, iu, c.L, amp, xs, acc, 71);
 }
 
 // Column phase, row id of a slab of WC staged columns: the down-hop part of
 // (H x)(id, c0 + c) into d[c].  ws: [ndn][WS] staged values, amp: down-hop
-// amplitudes by slot.
+// amplitudes by slot, L: the row's prefetched hop list.
 template <int WC, int WS>
 __device__ __forceinline__ void col_part(const DevSector& S, const double* __restrict__ ws,
-                                         const double* __restrict__ amp, int id, double (&d)[WC])
+                                         const double* __restrict__ amp, int id, const HopList& L, double (&d)[WC])
 {
 #pragma unroll
     for (int c = 0; c < WC; c++) d[c] = 0.0;
-    const int hd = __ldg(S.dn.hcnt + id);
-    for (int h = 0; h < hd; h++) {
-        const uint32_t e = hop_entry(S.dn, id, h);
-        EDZT_OK_OR(edzt_hop_rank(e) < S.dn.count && edzt_hop_slot(e) < S.dn.namp, 72, id, h, (long long)e, continue)
-        axpy_line<WC>(amp[edzt_hop_slot(e)], ws + edzt_hop_rank(e) * WS, d);
-    }
+    hop_sum<WC, WS>(S.dn, id, L, amp, ws, d, 72);
 }
 
 // Spin-flip and pair-hopping terms (impurity_hamiltonian.f90:179-226) of

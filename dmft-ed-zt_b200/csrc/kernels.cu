@@ -24,12 +24,14 @@ int kernels_debug_bad(long long* out4)
 // shared memory.
 // ---------------------------------------------------------------------------
 static constexpr int kHxThreads = 256;
+static constexpr int kHxThreadsLong = 1024;          // lines longer than kHxLongLine: one CTA per SM
+static constexpr int kHxLongLine = 4096;
 static constexpr size_t kHxSmemSoft = 100 * 1024;    // two CTAs per SM
 static constexpr size_t kHxSmemHard = 210 * 1024;    // one CTA per SM
 
 // Column phase: CTA b stages columns [b*WC, b*WC + WC) of every row.
-template <int WC>
-__global__ void __launch_bounds__(kHxThreads) k_hx_col(DevSector S, const double* __restrict__ x,
+template <int WC, int NT>
+__global__ void __launch_bounds__(NT) k_hx_col(DevSector S, const double* __restrict__ x,
                                                       double* __restrict__ D)
 {
     constexpr int WS = phase_stride(WC);
@@ -40,36 +42,28 @@ __global__ void __launch_bounds__(kHxThreads) k_hx_col(DevSector S, const double
     const int c0 = blockIdx.x * WC;
     stage_table(S.dn.amp, S.dn.namp, amp);
     const int n = ndn * WC;
-    for (int i0 = threadIdx.x; i0 < n; i0 += 4 * blockDim.x) {
-        double v[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int i = i0 + q * blockDim.x;
-            const int id = i / WC, c = i - id * WC;
-            v[q] = (i < n && c0 + c < nup) ? __ldg(x + (size_t)id * nup + c0 + c) : 0.0;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int i = i0 + q * blockDim.x;
-            const int id = i / WC, c = i - id * WC;
-            if (i < n) ws[id * WS + c] = v[q];
-        }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {   // the whole slab in flight at once
+        const int id = i / WC, c = i - id * WC;
+        const bool in = c0 + c < nup;
+        copy_async8(ws + id * WS + c, x + (in ? (size_t)id * nup + c0 + c : 0), in);
     }
+    copy_async_wait_all();
     __syncthreads();
+    HopList nxt{};
+    if ((int)threadIdx.x < ndn) nxt = hop_list(S.dn, threadIdx.x);
     for (int id = threadIdx.x; id < ndn; id += blockDim.x) {
+        const HopList cur = nxt;
+        if (id + (int)blockDim.x < ndn) nxt = hop_list(S.dn, id + blockDim.x);
         double d[WC];
-        col_part<WC, WS>(S, ws, amp, id, d);
-        double* out = D + (size_t)id * nup + c0;
-#pragma unroll
-        for (int c = 0; c < WC; c++)
-            if (c0 + c < nup) out[c] = d[c];
+        col_part<WC, WS>(S, ws, amp, id, cur, d);
+        store_slab_row<WC>(D, c0, ndn, id, d);          // columns past nup hold 0 (staged as 0)
     }
 }
 
 // Row phase: CTA b stages rows [b*R, b*R + R), thread per column.
-template <bool ACC, int R>
-__global__ void __launch_bounds__(kHxThreads) k_hx_row(DevSector S, const double* __restrict__ x,
-                                                      const double* __restrict__ D, double* __restrict__ y)
+template <bool ACC, int R, int NT>
+__global__ void __launch_bounds__(NT) k_hx_row(DevSector S, const double* __restrict__ x,
+                                                      const double* __restrict__ D, int wsh, double* __restrict__ y)
 {
     constexpr int RS = phase_stride(R);
     extern __shared__ __align__(16) double smem[];
@@ -81,12 +75,10 @@ __global__ void __launch_bounds__(kHxThreads) k_hx_row(DevSector S, const double
     const int nr = min(R, ndn - r0);
     stage_table(S.wint, S.P * S.P, wint);
     stage_table(S.up.amp, S.up.namp, amp);
-    for (int iu = threadIdx.x; iu < nup; iu += blockDim.x) {
-        double v[R];
+    for (int iu = threadIdx.x; iu < nup; iu += blockDim.x) {   // the whole tile in flight at once
 #pragma unroll
-        for (int r = 0; r < R; r++) v[r] = (r < nr) ? __ldg(x + (size_t)(r0 + r) * nup + iu) : 0.0;
-#pragma unroll
-        for (int r = 0; r < R; r++) xs[iu * RS + r] = v[r];
+        for (int r = 0; r < R; r++)
+            copy_async8(xs + iu * RS + r, x + (r < nr ? (size_t)(r0 + r) * nup + iu : 0), r < nr);
     }
     double e1d[R];
     int pd[R];
@@ -96,21 +88,25 @@ __global__ void __launch_bounds__(kHxThreads) k_hx_row(DevSector S, const double
         e1d[r] = __ldg(S.dn.e1 + id);
         pd[r] = __ldg(S.dn.imp + id);
     }
+    copy_async_wait_all();
     __syncthreads();
     auto fetch = [&](long long idx) {
         EDZT_OK_OR(idx >= 0 && idx < S.dim, 61, idx, S.dim, blockIdx.x, return 0.0)
         return __ldg(x + idx);
     };
+    RowCol<R> nxt{};
+    if ((int)threadIdx.x < nup) nxt = row_col<R>(S, D, wsh, threadIdx.x, r0, nr);
     for (int iu = threadIdx.x; iu < nup; iu += blockDim.x) {
+        const RowCol<R> cur = nxt;                          // this column's data; the next one's in flight
+        if (iu + (int)blockDim.x < nup) nxt = row_col<R>(S, D, wsh, iu + blockDim.x, r0, nr);
         double acc[R];
-        row_part<R, RS>(S, xs, wint, amp, iu, e1d, pd, acc);
-        const int pu = S.has_j ? (int)__ldg(S.up.imp + iu) : 0;
+        row_part<R, RS>(S, xs, wint, amp, iu, cur, e1d, pd, acc);
 #pragma unroll
         for (int r = 0; r < R; r++) {
             if (r >= nr) break;
             const size_t g = (size_t)(r0 + r) * nup + iu;
-            double v = acc[r] + __ldg(D + g);
-            if (S.has_j) v = exchange_part(S, r0 + r, iu, pu, pd[r], v, fetch);
+            double v = acc[r] + cur.dd[r];
+            if (S.has_j) v = exchange_part(S, r0 + r, iu, cur.pu, pd[r], v, fetch);
             y[g] = ACC ? y[g] + v : v;
         }
     }
@@ -150,30 +146,31 @@ bool hx_fits(int nup, int ndn)
     return row <= kHxSmemHard && col <= kHxSmemHard;
 }
 
-template <int R>
-static void launch_hx_row(const DevSector& S, const double* x, const double* D, double* y, int accumulate,
+template <int R, int NT>
+static void launch_hx_row(const DevSector& S, const double* x, const double* D, int wc, double* y, int accumulate,
                           cudaStream_t s)
 {
+    const int wsh = __builtin_ctz((unsigned)wc);
     static std::atomic<unsigned long long> attr_set{0};
     if (edzt_once_per_device(attr_set)) {
-        cudaFuncSetAttribute(k_hx_row<false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
-        cudaFuncSetAttribute(k_hx_row<true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
+        cudaFuncSetAttribute(k_hx_row<false, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
+        cudaFuncSetAttribute(k_hx_row<true, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
     }
     const int tiles = (S.dn.count + R - 1) / R;
     const size_t sm = (kWintDoubles + kAmpDoubles + (size_t)S.up.count * phase_stride(R)) * sizeof(double);
-    if (accumulate) k_hx_row<true, R><<<tiles, kHxThreads, sm, s>>>(S, x, D, y);
-    else k_hx_row<false, R><<<tiles, kHxThreads, sm, s>>>(S, x, D, y);
+    if (accumulate) k_hx_row<true, R, NT><<<tiles, NT, sm, s>>>(S, x, D, wsh, y);
+    else k_hx_row<false, R, NT><<<tiles, NT, sm, s>>>(S, x, D, wsh, y);
 }
 
-template <int W>
+template <int W, int NT>
 static void launch_hx_col(const DevSector& S, const double* x, double* D, cudaStream_t s)
 {
     static std::atomic<unsigned long long> attr_set{0};
     if (edzt_once_per_device(attr_set))
-        cudaFuncSetAttribute(k_hx_col<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
+        cudaFuncSetAttribute(k_hx_col<W, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
     const int slabs = (S.up.count + W - 1) / W;
     const size_t sm = (kAmpDoubles + (size_t)S.dn.count * phase_stride(W)) * sizeof(double);
-    k_hx_col<W><<<slabs, kHxThreads, sm, s>>>(S, x, D);
+    k_hx_col<W, NT><<<slabs, NT, sm, s>>>(S, x, D);
 }
 
 void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, double* scratch, cudaStream_t s)
@@ -183,17 +180,30 @@ void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, d
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    switch (hx_cols_of(nup, ndn, nsm)) {
-    case 16: launch_hx_col<16>(S, x, scratch, s); break;
-    case 8: launch_hx_col<8>(S, x, scratch, s); break;
-    case 4: launch_hx_col<4>(S, x, scratch, s); break;
-    default: launch_hx_col<2>(S, x, scratch, s); break;
+    // long lines (one CTA per SM) take 1024 threads, so the SM has 32 warps
+    // to overlap the hop lists' and neighbours' latency
+    const int wc = (ndn > kHxLongLine) ? (hx_cols_of(nup, ndn, nsm) == 4 ? 4 : 2) : hx_cols_of(nup, ndn, nsm);
+    if (ndn > kHxLongLine) {
+        if (wc == 4) launch_hx_col<4, kHxThreadsLong>(S, x, scratch, s);
+        else launch_hx_col<2, kHxThreadsLong>(S, x, scratch, s);
+    } else {
+        switch (wc) {
+        case 16: launch_hx_col<16, kHxThreads>(S, x, scratch, s); break;
+        case 8: launch_hx_col<8, kHxThreads>(S, x, scratch, s); break;
+        case 4: launch_hx_col<4, kHxThreads>(S, x, scratch, s); break;
+        default: launch_hx_col<2, kHxThreads>(S, x, scratch, s); break;
+        }
     }
-    switch (hx_rows_of(nup, ndn, nsm)) {
-    case 8: launch_hx_row<8>(S, x, scratch, y, accumulate, s); break;
-    case 4: launch_hx_row<4>(S, x, scratch, y, accumulate, s); break;
-    case 2: launch_hx_row<2>(S, x, scratch, y, accumulate, s); break;
-    default: launch_hx_row<1>(S, x, scratch, y, accumulate, s); break;
+    if (nup > kHxLongLine) {
+        if (hx_rows_of(nup, ndn, nsm) == 2) launch_hx_row<2, kHxThreadsLong>(S, x, scratch, wc, y, accumulate, s);
+        else launch_hx_row<1, kHxThreadsLong>(S, x, scratch, wc, y, accumulate, s);
+    } else {
+        switch (hx_rows_of(nup, ndn, nsm)) {
+        case 8: launch_hx_row<8, kHxThreads>(S, x, scratch, wc, y, accumulate, s); break;
+        case 4: launch_hx_row<4, kHxThreads>(S, x, scratch, wc, y, accumulate, s); break;
+        case 2: launch_hx_row<2, kHxThreads>(S, x, scratch, wc, y, accumulate, s); break;
+        default: launch_hx_row<1, kHxThreads>(S, x, scratch, wc, y, accumulate, s); break;
+        }
     }
 }
 

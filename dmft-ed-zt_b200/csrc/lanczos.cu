@@ -47,6 +47,7 @@ static constexpr int kRedDoubles = 32;
 static constexpr int kWintDoubles = EDZT_MAX_P * EDZT_MAX_P;
 static constexpr int kFixedDoubles = kRedDoubles + kWintDoubles + 2 * EDZT_MAX_AMP;
 static constexpr int kBarGroup = 16;                    // CTAs per barrier group
+static constexpr int kStageDepth = 16;                  // pair loads a thread keeps in flight when staging
 
 // sync words (unsigned), each counter on its own 128-byte line; SW_GEN is a
 // 64-bit word (barrier count << 32 | runs still going)
@@ -190,7 +191,11 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
     __syncthreads();
 
     // participant index of this CTA in phase ph of the current job
-    auto my_q = [&](int ph) { return (int)(((long long)blockIdx.x - sJ.ph[ph].tile0 % G + G) % G); };
+    auto my_q = [&](int ph) { return (int)blockIdx.x - sJ.ph[ph].part0; };
+    // this CTA's tiles of phase ph: [range[0], range[1])
+    auto my_range = [&](int ph) { return prefix + 2 * (size_t)(B.njobs + 1) + (size_t)ph * (G + 1) + blockIdx.x; };
+    // the slab that column-phase tile position t stages
+    const long long* __restrict__ slab_of = prefix + 2 * (size_t)(B.njobs + 1) + 2 * (size_t)(G + 1);
 
     // Sum of the current job's partial-sum slots of phase ph at parity par,
     // in participant order (every thread returns it).
@@ -305,32 +310,44 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
         const int c0 = tl * WC;
         double* ws = chunk;
         const int n = ndn * WC;
-        for (int i0 = threadIdx.x; i0 < n; i0 += 4 * T) {
-            double v[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int i = i0 + q * T;
+        if (k == 1) {
+            for (int i = threadIdx.x; i < n; i += T) {
                 const int id = i / WC, c = i - id * WC;
-                v[q] = (i < n && c0 + c < nup) ? form_v(sJ, k, pin, am, (long long)id * nup + c0 + c) : 0.0;
+                const double v = (c0 + c < nup) ? init_value(sJ, (long long)id * nup + c0 + c) : 0.0;
+                ws[id * WS + c] = v;
+                acc = fma(v, v, acc);
             }
+        } else {
+            // kStageDepth pair loads in flight per thread before the first is used
+            for (int i0 = threadIdx.x; i0 < n; i0 += kStageDepth * T) {
+                double2 pr[kStageDepth];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int i = i0 + q * T;
-                const int id = i / WC, c = i - id * WC;
-                if (i < n) {
-                    ws[id * WS + c] = v[q];
-                    acc = fma(v[q], v[q], acc);
+                for (int q = 0; q < kStageDepth; q++) {
+                    const int i = i0 + q * T;
+                    const int id = i / WC, c = i - id * WC;
+                    pr[q] = (i < n && c0 + c < nup) ? __ldcg(pin + (long long)id * nup + c0 + c) : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int q = 0; q < kStageDepth; q++) {
+                    const int i = i0 + q * T;
+                    const int id = i / WC, c = i - id * WC;
+                    if (i < n) {
+                        const double v = fma(am, pr[q].y, pr[q].x);   // form_v of the stored pair
+                        ws[id * WS + c] = v;
+                        acc = fma(v, v, acc);
+                    }
                 }
             }
         }
         __syncthreads();
+        HopList nxt{};
+        if ((int)threadIdx.x < ndn) nxt = hop_list(sJ.S.dn, threadIdx.x);
         for (int id = threadIdx.x; id < ndn; id += T) {
+            const HopList cur = nxt;                     // this row's hop list; the next one's in flight
+            if (id + T < ndn) nxt = hop_list(sJ.S.dn, id + T);
             double d[WC];
-            col_part<WC, WS>(sJ.S, ws, amp_dn, id, d);
-            double* out = sJ.D + (long long)id * nup + c0;
-#pragma unroll
-            for (int c = 0; c < WC; c++)
-                if (c0 + c < nup) __stcg(out + c, d[c]);
+            col_part<WC, WS>(sJ.S, ws, amp_dn, id, cur, d);
+            store_slab_row<WC>(sJ.D, c0, ndn, id, d);   // columns past nup hold 0 (staged as 0)
         }
         __syncthreads();
     };
@@ -349,6 +366,7 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
         const bool coeff = (sJ.mode == LZ_COEFF);
         const double ck = coeff ? 0.0 : sJ.coeff[k - 1];
         const int r0 = tl * R, nr = min(R, ndn - r0);
+        const int wsh = __ffs(sJ.ph[0].width) - 1;       // D's slab width, log2
         double* xs = chunk;                              // [nup][RS] w_k
         double* ps = chunk + nup * RS;                   // [nup][RS] w_{k-1}
         // w at a global index, as its owner forms it (exchange terms)
@@ -357,26 +375,38 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
             const double v = form_v(sJ, k, pin, am, idx);
             return first ? v / n0 : v * rb;
         };
-        for (int iu = threadIdx.x; iu < nup; iu += T) {
-            double w[R], wp[R];
+        if (first) {
+            for (int iu = threadIdx.x; iu < nup; iu += T) {
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                w[r] = wp[r] = 0.0;
-                if (r < nr) {
+                for (int r = 0; r < R; r++) {
                     const long long e = (long long)(r0 + r) * nup + iu;
-                    if (first) {
-                        w[r] = init_value(sJ, e) / n0;   // the reference divides (:130)
-                    } else {
-                        const double2 pr = __ldcg(pin + e);
-                        w[r] = fma(am, pr.y, pr.x) * rb;
-                        wp[r] = pr.y;
-                    }
+                    xs[iu * RS + r] = (r < nr) ? init_value(sJ, e) / n0 : 0.0;   // the reference divides (:130)
+                    ps[iu * RS + r] = 0.0;
                 }
             }
+        } else {
+            // U columns of R rows per thread: U * R pair loads in flight before the first is used
+            constexpr int U = (kStageDepth / R) > 0 ? kStageDepth / R : 1;
+            for (int iu0 = threadIdx.x; iu0 < nup; iu0 += U * T) {
+                double2 pr[U][R];
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                xs[iu * RS + r] = w[r];
-                ps[iu * RS + r] = wp[r];
+                for (int u = 0; u < U; u++) {
+                    const int iu = iu0 + u * T;
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                        pr[u][r] = (iu < nup && r < nr) ? __ldcg(pin + (long long)(r0 + r) * nup + iu)
+                                                        : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int iu = iu0 + u * T;
+                    if (iu >= nup) break;
+#pragma unroll
+                    for (int r = 0; r < R; r++) {
+                        xs[iu * RS + r] = fma(am, pr[u][r].y, pr[u][r].x) * rb;
+                        ps[iu * RS + r] = pr[u][r].y;
+                    }
+                }
             }
         }
         double e1d[R];
@@ -388,17 +418,19 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
             pd[r] = __ldg(sJ.S.dn.imp + id);
         }
         __syncthreads();
+        RowCol<R> nxt{};
+        if ((int)threadIdx.x < nup) nxt = row_col<R>(sJ.S, sJ.D, wsh, threadIdx.x, r0, nr);
         for (int iu = threadIdx.x; iu < nup; iu += T) {
+            const RowCol<R> cur = nxt;                   // this column's data; the next one's in flight
+            if (iu + T < nup) nxt = row_col<R>(sJ.S, sJ.D, wsh, iu + T, r0, nr);
             double hv[R];
-            row_part<R, RS>(sJ.S, xs, wint, amp_up, iu, e1d, pd, hv);
-            const int pu = sJ.S.has_j ? (int)__ldg(sJ.S.up.imp + iu) : 0;
+            row_part<R, RS>(sJ.S, xs, wint, amp_up, iu, cur, e1d, pd, hv);
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 if (r >= nr) break;
                 const long long e = (long long)(r0 + r) * nup + iu;
-                const double dd = __ldcg(sJ.D + e);
-                double y = hv[r] + (first ? dd / n0 : dd * rb);
-                if (sJ.S.has_j) y = exchange_part(sJ.S, r0 + r, iu, pu, pd[r], y, fetch_w);
+                double y = hv[r] + (first ? cur.dd[r] / n0 : cur.dd[r] * rb);
+                if (sJ.S.has_j) y = exchange_part(sJ.S, r0 + r, iu, cur.pu, pd[r], y, fetch_w);
                 const double w = xs[iu * RS + r];
                 if (!first) y = fma(-bk, ps[iu * RS + r], y);
                 __stcg(pout + e, make_double2(y, w));
@@ -418,9 +450,11 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
     for (; p < B.max_phases; p++) {
         const int ph = p & 1;
         const long long* pre = prefix + (size_t)ph * (B.njobs + 1);
+        const long long* rg = my_range(ph);
+        const long long t_end = __ldg(rg + 1);
         int cur = -1;
         double acc = 0.0;
-        for (long long t = blockIdx.x; t < B.total[ph]; t += G) {
+        for (long long t = __ldg(rg); t < t_end; t++) {
             if (cur < 0 || t >= __ldg(pre + cur + 1)) {
                 if (cur >= 0 && sS.active) flush(ph, acc);
                 cur = find_job(pre, B.njobs, t);
@@ -428,18 +462,16 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
                 acc = 0.0;
             }
             if (!sS.active) continue;
-            const int tl = (int)(t - sJ.ph[ph].tile0);
+            const int tl = (ph == 0) ? (int)__ldg(slab_of + t) : (int)(t - sJ.ph[ph].tile0);
             const int wdt = sJ.ph[ph].width;
             if (ph == 0) {
                 switch (wdt) {
-                case 16: col_tile(std::integral_constant<int, 16>{}, tl, acc); break;
                 case 8: col_tile(std::integral_constant<int, 8>{}, tl, acc); break;
                 case 4: col_tile(std::integral_constant<int, 4>{}, tl, acc); break;
                 default: col_tile(std::integral_constant<int, 2>{}, tl, acc); break;
                 }
             } else {
                 switch (wdt) {
-                case 8: row_tile(std::integral_constant<int, 8>{}, tl, acc); break;
                 case 4: row_tile(std::integral_constant<int, 4>{}, tl, acc); break;
                 case 2: row_tile(std::integral_constant<int, 2>{}, tl, acc); break;
                 default: row_tile(std::integral_constant<int, 1>{}, tl, acc); break;
@@ -452,8 +484,10 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
     }
     if (B.slice && running != 0u && p == B.max_phases) {  // budget spent: open every run's next step
         const long long* pre = prefix;
+        const long long* rg = my_range(0);
+        const long long t_end = __ldg(rg + 1);
         int cur = -1;
-        for (long long t = blockIdx.x; t < B.total[0]; t += G) {
+        for (long long t = __ldg(rg); t < t_end; t++) {
             if (cur < 0 || t >= __ldg(pre + cur + 1)) {
                 cur = find_job(pre, B.njobs, t);
                 begin_job(cur, p, true);
@@ -494,6 +528,8 @@ cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, const
 // Per-CTA dynamic shared memory: two CTAs of 256 threads per SM when every
 // job fits, else one CTA of 512 threads per SM.
 static constexpr size_t kLzSmemTwoPerSm = 108 * 1024;
+// Fixed cost of a tile in states, for cutting the tile list into CTA ranges
+static constexpr double kLzTileCost = 8192.0;
 
 // Width (of opts, descending) for `count` lines, each tile needing need(w)
 // bytes of the budget: with few tiles in the launch, the one that minimises
@@ -533,7 +569,7 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, 
     const size_t budget = (two ? kLzSmemTwoPerSm : kLzSmemMax) - fixed;
     const int G_est = (two ? 2 : 1) * nsm;
     const bool many = lines8 >= 4LL * G_est;
-    const int ropts[4] = {8, 4, 2, 1}, copts[4] = {16, 8, 4, 2};
+    const int ropts[3] = {4, 2, 1}, copts[3] = {8, 4, 2};
     size_t chunk = 0;
     for (int j = 0; j < nj; j++) {
         LzJob& J = jobs[j];
@@ -541,16 +577,17 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, 
         // a width preset by the tuner is kept when it fits this launch's budget
         const int wc = J.ph[0].width, r = J.ph[1].width;
         J.ph[0].width = (wc > 0 && lz_col_smem(ndn, wc) <= budget)
-                            ? wc : pick_width(copts, 4, nup, budget, G_est, many, [&](int w) { return lz_col_smem(ndn, w); });
+                            ? wc : pick_width(copts, 3, nup, budget, G_est, many, [&](int w) { return lz_col_smem(ndn, w); });
         J.ph[1].width = (r > 0 && lz_row_smem(nup, r) <= budget)
-                            ? r : pick_width(ropts, 4, ndn, budget, G_est, many, [&](int w) { return lz_row_smem(nup, w); });
+                            ? r : pick_width(ropts, 3, ndn, budget, G_est, many, [&](int w) { return lz_row_smem(nup, w); });
         chunk = std::max(chunk, std::max(lz_col_smem(ndn, J.ph[0].width), lz_row_smem(nup, J.ph[1].width)));
     }
     P.smem = fixed + chunk;
     P.grid = lz_grid_size(device, P.smem, P.block);
     if (P.grid <= 0) return P;
     const int G = P.grid;
-    prefix.assign(2 * (size_t)(nj + 1), 0);
+    prefix.assign(2 * (size_t)(nj + 1) + 2 * (size_t)(G + 1), 0);
+    std::vector<long long> slab_order;
     for (int ph = 0; ph < 2; ph++) {
         long long* pre = prefix.data() + (size_t)ph * (nj + 1);
         for (int j = 0; j < nj; j++) {
@@ -559,11 +596,67 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, 
             Q.ntiles = (count + Q.width - 1) / Q.width;
             Q.tile0 = pre[j];
             pre[j + 1] = pre[j] + Q.ntiles;
-            Q.npart = std::min(G, Q.ntiles);
+        }
+        const long long T = pre[nj];
+        P.total[ph] = T;
+        // CTA ranges: with no more tiles than CTAs, CTA b takes tile b; else
+        // the list is cut where the running cost crosses b/G of the total
+        // (a tile costs its states plus a fixed amount for its staging round
+        // and barriers), every CTA keeping at least one tile.
+        long long* range = prefix.data() + 2 * (size_t)(nj + 1) + (size_t)ph * (G + 1);
+        if (T <= G) {
+            for (int b = 0; b <= G; b++) range[b] = std::min<long long>(b, T);
+        } else {
+            std::vector<double> cum((size_t)T + 1, 0.0);
+            for (int j = 0; j < nj; j++) {
+                const LzPhase& Q = jobs[j].ph[ph];
+                const long long lines = (ph == 0) ? jobs[j].S.dn.count : jobs[j].S.up.count;
+                const int count = (ph == 0) ? jobs[j].S.up.count : jobs[j].S.dn.count;
+                for (int i = 0; i < Q.ntiles; i++) {
+                    const int w = std::min(Q.width, count - i * Q.width);
+                    cum[Q.tile0 + i + 1] = cum[Q.tile0 + i] + (double)lines * w + kLzTileCost;
+                }
+            }
+            range[0] = 0;
+            range[G] = T;
+            long long t = 0;
+            for (int b = 1; b < G; b++) {
+                const double target = cum[T] * b / G;
+                while (t < T && cum[t + 1] <= target) t++;
+                range[b] = std::min(std::max(t, range[b - 1] + 1), T - (G - b));
+                t = range[b];
+            }
+        }
+        // participants of a job: the CTAs whose range meets its tiles (a contiguous run)
+        auto owner = [&](long long tile) {
+            return (int)(std::upper_bound(range, range + G + 1, tile) - range) - 1;
+        };
+        for (int j = 0; j < nj; j++) {
+            LzPhase& Q = jobs[j].ph[ph];
+            Q.part0 = owner(Q.tile0);
+            Q.npart = owner(Q.tile0 + Q.ntiles - 1) - Q.part0 + 1;
             Q.slot0 = P.slots;
             P.slots += Q.npart;
         }
-        P.total[ph] = pre[nj];
+        // Column phase: the slab each tile position stages.  A participant
+        // takes its positions in order; numbering the slabs by round (the
+        // r-th tile of every participant, participants in order) makes the
+        // participants stage neighbouring slabs at the same time, so the
+        // rows they read sit side by side in DRAM.
+        if (ph == 0) {
+            slab_order.assign((size_t)T, 0);
+            for (int j = 0; j < nj; j++) {
+                const LzPhase& Q = jobs[j].ph[0];
+                const long long lo = Q.tile0, hi = Q.tile0 + Q.ntiles;
+                long long next = 0;
+                for (long long r = 0; next < Q.ntiles; r++)
+                    for (int q = 0; q < Q.npart; q++) {
+                        const long long s0 = std::max(range[Q.part0 + q], lo), s1 = std::min(range[Q.part0 + q + 1], hi);
+                        if (s0 + r < s1) slab_order[(size_t)(s0 + r)] = next++;
+                    }
+            }
+        }
     }
+    prefix.insert(prefix.end(), slab_order.begin(), slab_order.end());
     return P;
 }

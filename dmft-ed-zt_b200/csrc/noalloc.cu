@@ -8,7 +8,7 @@
 // call uses no device memory but the scratch array below and the context's
 // model tables, which an earlier allocating call on the same sector built.
 //
-// Scratch: one file-scope __device__ array of kNoAllocScratchBytes (10.1 MiB)
+// Scratch: one file-scope __device__ array of kNoAllocScratchBytes (13.1 MiB)
 // that every GPU which loads the library holds until the process exits.  It
 // limits the sector to EDZT_NOALLOC_MAX_DIM states and the run to
 // EDZT_NOALLOC_MAX_STEPS steps.  The first call on each device looks the
@@ -39,7 +39,9 @@ constexpr size_t al(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 constexpr size_t kOffJob = 0;
 constexpr size_t kOffState = kOffJob + al(2048);        // LzJob
 constexpr size_t kOffPrefix = kOffState + al(2 * sizeof(LzState));
-constexpr size_t kOffStatus = kOffPrefix + al(4 * sizeof(long long));
+// the jobs' first tiles, the CTA ranges and the column phase's slab order
+// (at most one slab per two up strings)
+constexpr size_t kOffStatus = kOffPrefix + al((4 + 2 * (kMaxGrid + 1) + EDZT_NOALLOC_MAX_DIM / 2) * sizeof(long long));
 constexpr size_t kOffSync = kOffStatus + al(sizeof(int));
 constexpr size_t kSyncBytes = al(sizeof(unsigned) * (128 + 32 * ((kMaxGrid + 15) / 16)));
 constexpr size_t kOffSlots = kOffSync + kSyncBytes;     // [2 phases * kMaxGrid][2] doubles
@@ -47,7 +49,10 @@ constexpr size_t kOffAB = kOffSlots + al(sizeof(double) * 4 * kMaxGrid);
 constexpr size_t kOffYW = kOffAB + al(sizeof(double) * 2 * EDZT_NOALLOC_MAX_STEPS);
 constexpr size_t kYWBytes = sizeof(double2) * (size_t)EDZT_NOALLOC_MAX_DIM;
 constexpr size_t kOffD = kOffYW + 2 * kYWBytes;
-constexpr size_t kNoAllocScratchBytes = kOffD + sizeof(double) * (size_t)EDZT_NOALLOC_MAX_DIM;
+// D is slab-major with slabs of up to 8 columns: up to 7 padding columns of
+// every row past the sector's own states
+constexpr size_t kDDoubles = 2 * (size_t)EDZT_NOALLOC_MAX_DIM;
+constexpr size_t kNoAllocScratchBytes = kOffD + sizeof(double) * kDDoubles;
 
 static_assert(sizeof(LzJob) <= 2048, "job descriptor outgrew its scratch slot");
 
@@ -156,6 +161,8 @@ void run(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, 
     const LzPlan P = lz_plan(device, &J, 1, prefix);
     if (P.grid <= 0) throw Fail{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
     if (P.grid > kMaxGrid) throw Fail{EDZT_ERR_CUDA, "persistent grid larger than the no-allocation sync area"};
+    if ((size_t)J.ph[0].ntiles * J.ph[0].width * S.dn.count > kDDoubles)
+        throw Fail{EDZT_ERR_ARG, "sector's column slabs exceed the no-allocation scratch"};
     // The start vector is read in the first step only (both phases), which
     // writes YW[1]; a host vector is staged in YW[0], first written by step 2.
     if (is_device_ptr(v_init, device)) {

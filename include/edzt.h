@@ -108,7 +108,7 @@ int edzt_lanczos_iteration(edzt_ctx *ctx, int ne_up, int ne_dn, const double *v_
  * owned entirely by another allocator, or a latency-critical loop that must
  * not take the device-wide synchronisation an allocation can cause.  Same
  * arguments and results as edzt_lanczos_iteration, always on the persistent
- * kernel, whose scratch is one static device array of about 10.1 MiB that
+ * kernel, whose scratch is one static device array of about 13.1 MiB that
  * every GPU loading the library holds until exit.  Limits: sector dimension
  * <= EDZT_NOALLOC_MAX_DIM, maxnstep <= EDZT_NOALLOC_MAX_STEPS (EDZT_ERR_ARG
  * beyond).  The sector's tables must already exist on the context (built by

@@ -159,7 +159,20 @@ def test_solve_aim_n12(solver, configs, oracle_mod):
     """The large single-solve workload (nsite 12, 9 sectors, 300 steps) end
     to end: E0, G(i w_n) on 2048 points, and the first 50 continued-fraction
     coefficients a_n, b_n of the c^+ and the c run (src/dmft_green.f90:204-250;
-    excitation sectors of 731,808 states)."""
+    excitation sectors of 731,808 states).
+
+    The coefficients are compared on the same start vector, c^(+) applied to
+    the library's ground state: the two implementations' ground states each
+    come out of a 300-step Lanczos run and its eigenvector pass and agree to
+    about 1e-9, and these c^(+) runs amplify a start-vector difference fast
+    (measured on the oracle alone: a 1-ulp perturbation of c^+|gs> moves a_n
+    by 1e-12 at step 16, 1e-10 at step 29 and 1e-8 at step 56), so runs from
+    the two ground states separate before step 50 whatever the arithmetic.
+    From the same start vector the runs still differ by the rounding of
+    their sums (another order of the same terms), amplified the same way:
+    measured on a B200, at most 1.7e-9 over the first 35 coefficients and
+    3.4e-8 over the first 50.  The test holds the first 35 to 1e-8 and the
+    first 50 to 1e-7."""
     cfg = configs.aim_n12()
     o = oracle_for(oracle_mod, cfg["model"])
     gs_ref = o.ground_state(cfg["sectors"], cfg["maxnstep"], seed=0)
@@ -172,14 +185,17 @@ def test_solve_aim_n12(solver, configs, oracle_mod):
     assert np.abs(r["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
     gs = solver.ground_state(cfg["sectors"], cfg["maxnstep"], seed=0)
     assert gs["isector"] == gs_ref["isector"]
+    assert abs(abs(gs["vec"] @ gs_ref["vec"]) - 1.0) <= 1e-8
     cg = solver.cluster_green_ftn(1, cfg["maxnstep"], omega)
     assert np.abs(cg["G_cl"] - cg_ref["G_cl"]).max() <= G_TOL
-    c, cr = cg["coeffs"], cg_ref["coeffs"]
+    same_start = o.cluster_green_ftn(1, nu, nd, gs["vec"], gs["e0"], cfg["maxnstep"], omega[:8])
+    c, cr = cg["coeffs"], same_start["coeffs"]
     for q in (0, 2):                       # (a^+, b^+) and (a^-, b^-) of the impurity orbital, spin up
         k = ab_compare_len(cr[0, 0, q + 1], cfg["maxnstep"])
         assert k == 50
-        assert np.abs(c[0, 0, q, :k] - cr[0, 0, q, :k]).max() <= AB_TOL
-        assert np.abs(c[0, 0, q + 1, :k] - cr[0, 0, q + 1, :k]).max() <= AB_TOL
+        for kk, tol in ((35, AB_TOL), (50, 10 * AB_TOL)):
+            assert np.abs(c[0, 0, q, :kk] - cr[0, 0, q, :kk]).max() <= tol
+            assert np.abs(c[0, 0, q + 1, :kk] - cr[0, 0, q + 1, :kk]).max() <= tol
 
 
 @pytest.mark.parametrize("nspin", [1, 2])
