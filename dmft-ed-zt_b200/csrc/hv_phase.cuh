@@ -140,27 +140,34 @@ __device__ __forceinline__ void store_slab_row(double* __restrict__ D, int c0, i
 }
 
 // What the row phase reads from global memory for column iu of a tile of R
-// rows: the column's up string (energy, impurity bits, hop list) and the
-// down-hop part D of its R elements (slabs of 2^wsh columns); loaded one
-// column ahead.
+// rows: the column's up string (energy, impurity bits, hop list), the
+// down-hop part D of its R elements (slabs of 2^wsh columns) and, in the
+// Lanczos kernel, w_{k-1} of those elements (the second value of each stored
+// (y, w) pair; prev null: none); loaded one column ahead.
 template <int R>
 struct RowCol {
     double e1u;
     int pu;
     HopList L;
     double dd[R];
+    double wp[R];
 };
 
 template <int R>
 __device__ __forceinline__ RowCol<R> row_col(const DevSector& S, const double* __restrict__ D, int wsh, int iu,
-                                             int r0, int nr)
+                                             int r0, int nr, const double2* __restrict__ prev = nullptr)
 {
     RowCol<R> c;
     c.e1u = __ldg(S.up.e1 + iu);
     c.pu = __ldg(S.up.imp + iu);
     c.L = hop_list(S.up, iu);
 #pragma unroll
-    for (int r = 0; r < R; r++) c.dd[r] = (r < nr) ? __ldcg(D + slab_index(r0 + r, iu, S.dn.count, wsh)) : 0.0;
+    for (int r = 0; r < R; r++) {
+        c.dd[r] = (r < nr) ? __ldcg(D + slab_index(r0 + r, iu, S.dn.count, wsh)) : 0.0;
+        c.wp[r] = (prev != nullptr && r < nr)
+                      ? __ldcg(reinterpret_cast<const double*>(prev + (long long)(r0 + r) * S.up.count + iu) + 1)
+                      : 0.0;
+    }
     return c;
 }
 

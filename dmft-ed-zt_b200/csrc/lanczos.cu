@@ -43,7 +43,7 @@
 #include "hv_phase.cuh"
 
 static constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000ull * 1000ull * 1000ull;
-static constexpr int kRedDoubles = 32;
+static constexpr int kRedDoubles = 64;
 static constexpr int kWintDoubles = EDZT_MAX_P * EDZT_MAX_P;
 static constexpr int kFixedDoubles = kRedDoubles + kWintDoubles + 2 * EDZT_MAX_AMP;
 static constexpr int kBarGroup = 16;                    // CTAs per barrier group
@@ -58,7 +58,7 @@ static constexpr int kStageDepth = 16;                  // pair loads a thread k
 
 size_t lz_sync_bytes(int G) { return sizeof(unsigned) * (128 + 32 * (size_t)((G + kBarGroup - 1) / kBarGroup)); }
 
-size_t lz_row_smem(int nup, int R) { return 2 * (size_t)nup * phase_stride(R) * sizeof(double); }
+size_t lz_row_smem(int nup, int R) { return (size_t)nup * phase_stride(R) * sizeof(double); }
 size_t lz_col_smem(int ndn, int WC) { return (size_t)ndn * phase_stride(WC) * sizeof(double); }
 size_t lz_fixed_smem() { return kFixedDoubles * sizeof(double); }
 
@@ -197,14 +197,6 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
     // the slab that column-phase tile position t stages
     const long long* __restrict__ slab_of = prefix + 2 * (size_t)(B.njobs + 1) + 2 * (size_t)(G + 1);
 
-    // Sum of the current job's partial-sum slots of phase ph at parity par,
-    // in participant order (every thread returns it).
-    auto slot_sum = [&](int ph, int par) {
-        double v[1] = {0.0};
-        for (int i = threadIdx.x; i < sJ.ph[ph].npart; i += T) v[0] += __ldcg(slots + (sJ.ph[ph].slot0 + i) * 2 + par);
-        block_sum<1>(v, red);
-        return v[0];
-    };
 
     // Enter job j in phase p: load it if needed and derive its state.  The
     // closing pass of a slice (closing) opens the next step only: it derives
@@ -223,6 +215,19 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
             if (threadIdx.x == 0) s_job = j;
         }
         const int ph = p & 1;
+        // The sums of the other phase's partial-sum slots, both parities, in
+        // participant order (every thread gets them), loaded while thread 0
+        // loads the run's state: which parity applies depends on the step.
+        double ps2[2] = {0.0, 0.0};
+        {
+            const LzPhase& O = sJ.ph[ph ^ 1];
+            const double2* sl = reinterpret_cast<const double2*>(slots) + O.slot0;
+            for (int i = threadIdx.x; i < O.npart; i += T) {
+                const double2 q = __ldcg(sl + i);
+                ps2[0] += q.x;
+                ps2[1] += q.y;
+            }
+        }
         if (threadIdx.x == 0) {
             const int* ss = reinterpret_cast<const int*>(sJ.st + ((p + 1) & 1));
             int* sd = reinterpret_cast<int*>(&sS);
@@ -231,7 +236,7 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
             if (ph == 0 && !sS.opened) sS.k += 1;        // the column phase opens the next step
             sS.opened = 0;
         }
-        __syncthreads();
+        block_sum<2>(ps2, red);                          // ends with a CTA barrier: sS is visible
         if (s_resumed) {
             if (threadIdx.x == 0 && my_q(0) == 0) sJ.st[p & 1] = sS;
             __syncthreads();
@@ -244,7 +249,7 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
         // but sums ||v_init|| itself)
         double sum = 0.0;
         if (sS.active && ((ph == 0 && k >= 2 && coeff) || (ph == 1 && (coeff || k == 1))))
-            sum = (ph == 0) ? slot_sum(1, (k - 1) & 1) : slot_sum(0, k & 1);
+            sum = (ph == 0) ? ps2[(k - 1) & 1] : ps2[k & 1];
         if (threadIdx.x == 0) {
             const bool out = (my_q(ph) == 0);
             LzState n = sS;
@@ -368,7 +373,7 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
         const int r0 = tl * R, nr = min(R, ndn - r0);
         const int wsh = __ffs(sJ.ph[0].width) - 1;       // D's slab width, log2
         double* xs = chunk;                              // [nup][RS] w_k
-        double* ps = chunk + nup * RS;                   // [nup][RS] w_{k-1}
+        const double2* prev = first ? nullptr : pin;     // w_{k-1}: read with each column's data
         // w at a global index, as its owner forms it (exchange terms)
         auto fetch_w = [&](long long idx) {
             EDZT_OK_OR(idx >= 0 && idx < sJ.S.dim, 21, idx, sJ.S.dim, k, return 0.0)
@@ -381,7 +386,6 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
                 for (int r = 0; r < R; r++) {
                     const long long e = (long long)(r0 + r) * nup + iu;
                     xs[iu * RS + r] = (r < nr) ? init_value(sJ, e) / n0 : 0.0;   // the reference divides (:130)
-                    ps[iu * RS + r] = 0.0;
                 }
             }
         } else {
@@ -402,10 +406,7 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
                     const int iu = iu0 + u * T;
                     if (iu >= nup) break;
 #pragma unroll
-                    for (int r = 0; r < R; r++) {
-                        xs[iu * RS + r] = fma(am, pr[u][r].y, pr[u][r].x) * rb;
-                        ps[iu * RS + r] = pr[u][r].y;
-                    }
+                    for (int r = 0; r < R; r++) xs[iu * RS + r] = fma(am, pr[u][r].y, pr[u][r].x) * rb;
                 }
             }
         }
@@ -419,10 +420,10 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
         }
         __syncthreads();
         RowCol<R> nxt{};
-        if ((int)threadIdx.x < nup) nxt = row_col<R>(sJ.S, sJ.D, wsh, threadIdx.x, r0, nr);
+        if ((int)threadIdx.x < nup) nxt = row_col<R>(sJ.S, sJ.D, wsh, threadIdx.x, r0, nr, prev);
         for (int iu = threadIdx.x; iu < nup; iu += T) {
             const RowCol<R> cur = nxt;                   // this column's data; the next one's in flight
-            if (iu + T < nup) nxt = row_col<R>(sJ.S, sJ.D, wsh, iu + T, r0, nr);
+            if (iu + T < nup) nxt = row_col<R>(sJ.S, sJ.D, wsh, iu + T, r0, nr, prev);
             double hv[R];
             row_part<R, RS>(sJ.S, xs, wint, amp_up, iu, cur, e1d, pd, hv);
 #pragma unroll
@@ -432,7 +433,7 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
                 double y = hv[r] + (first ? cur.dd[r] / n0 : cur.dd[r] * rb);
                 if (sJ.S.has_j) y = exchange_part(sJ.S, r0 + r, iu, cur.pu, pd[r], y, fetch_w);
                 const double w = xs[iu * RS + r];
-                if (!first) y = fma(-bk, ps[iu * RS + r], y);
+                if (!first) y = fma(-bk, cur.wp[r], y);
                 __stcg(pout + e, make_double2(y, w));
                 if (coeff) {
                     acc = fma(w, y, acc);
@@ -529,7 +530,7 @@ cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, const
 // job fits, else one CTA of 512 threads per SM.
 static constexpr size_t kLzSmemTwoPerSm = 108 * 1024;
 // Fixed cost of a tile in states, for cutting the tile list into CTA ranges
-static constexpr double kLzTileCost = 8192.0;
+static constexpr double kLzTileCost = 1024.0;
 
 // Width (of opts, descending) for `count` lines, each tile needing need(w)
 // bytes of the budget: with few tiles in the launch, the one that minimises

@@ -161,7 +161,7 @@ void run(edzt_ctx* c, int ne_up, int ne_dn, const double* v_init, int maxnstep, 
     const LzPlan P = lz_plan(device, &J, 1, prefix);
     if (P.grid <= 0) throw Fail{EDZT_ERR_CUDA, "persistent kernel cannot be resident (shared memory too large)"};
     if (P.grid > kMaxGrid) throw Fail{EDZT_ERR_CUDA, "persistent grid larger than the no-allocation sync area"};
-    if ((size_t)J.ph[0].ntiles * J.ph[0].width * S.dn.count > kDDoubles)
+    if ((size_t)((S.up.count + J.ph[0].width - 1) / J.ph[0].width) * J.ph[0].width * S.dn.count > kDDoubles)
         throw Fail{EDZT_ERR_ARG, "sector's column slabs exceed the no-allocation scratch"};
     // The start vector is read in the first step only (both phases), which
     // writes YW[1]; a host vector is staged in YW[0], first written by step 2.
