@@ -566,6 +566,9 @@ def run_gpu(args):
     clk = clocks.stop()
     launches = s.launch_count() - launches0
     ks = s.kernel_stats()
+    # whether the solves ran an eigenvector pass (a launch over the winning
+    # sector alone) or took the eigenvector from the scan's kept pairs
+    eig_pass = any(e["states"] in [float(s.dim(u, d)) for u, d in sectors] for e in s.launch_log())
     total_ms = sum(lat)
     replicas = importlib.import_module("dmft_ed_zt_b200.replicas")
     total_ms = replicas.max_over_ranks(total_ms, dist, device="cuda")
@@ -623,12 +626,13 @@ def run_gpu(args):
         s.set_engine(pkg.ENGINE_FUSED)
         # Lanczos state-steps of a solve in each engine: the plain engine runs
         # the eigenvector pass of every sector as the reference does, the
-        # fused engine only the winner's, so part of the ratio is skipped work
+        # fused engine only the winner's (or none: the eigenvector from the
+        # scan's kept pairs), so part of the ratio is skipped work
         dims = [s.dim(u, d) for u, d in sectors]
         gdim = sum(s.dim(u + du, d + dd) for (u, d) in [max(sectors, key=lambda q: s.dim(*q))]
                    for du, dd in ((1, 0), (-1, 0)))
         plain_steps = sum(2 * maxn * x for x in dims) + maxn * gdim
-        fused_steps = sum(maxn * x for x in dims) + maxn * max(dims) + maxn * gdim
+        fused_steps = sum(maxn * x for x in dims) + (maxn * max(dims) if eig_pass else 0) + maxn * gdim
         ratio = (1000.0 * len(pl) / sum(pl))
         plain = {"value": ratio, "unit": UNIT, "ms_per_solve": sum(pl) / len(pl),
                  "engine": "one kernel per BLAS-1 step + H.v kernels, host reads of every reduction, "
@@ -644,25 +648,34 @@ def run_gpu(args):
                 "kernel": "k_lanczos (persistent fused Lanczos)", "peak_source": peak_src,
                 "launches": ks["launches"], "avg_launch_ms": ks["ms"] / max(ks["launches"], 1),
                 "algorithmic_bytes_per_launch": ks["bytes"] / max(ks["launches"], 1),
+                "eigenvector": "eigenvector pass" if eig_pass else "from the scan's kept Lanczos pairs",
                 "note": "24 B/state per coefficient step, 40 B/state per eigenvector step; the "
-                        "ground-state batch (9 sectors, 245 MB of vectors) exceeds L2, the eigenvector "
-                        "and Green's-function launches (<= 27 MB) are L2-resident"}
+                        "ground-state scan (9 sectors, 252 MB of pair buffers and D) exceeds L2, the "
+                        "eigenvector and Green's-function launches are L2-resident"}
     roofline["traffic"] = read_traffic(args.traffic_file)
-    # the launches of one solve separately: ground-state scan, eigenvector
-    # pass, c/c^+ runs (each timed solve makes these three, in this order)
+    # the launches of one solve separately, told apart by the states they
+    # carry: the ground-state scan (every sector), the eigenvector pass of the
+    # winner (absent when the scan kept its Lanczos pairs), the c/c^+ runs
     log = s.launch_log()
-    names = ["ground-state scan (9 sectors, 300 steps)", "eigenvector pass (winning sector)",
-             "c / c^+ runs (2 excitation sectors, 300 steps)"]
-    if log and len(log) % 3 == 0:
-        per = []
-        for q in range(3):
-            ent = log[q::3]
-            ms = sum(e["ms"] for e in ent) / len(ent)
-            by = sum(e["bytes"] for e in ent) / len(ent)
-            gbs = by / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
-            per.append({"launch": names[q], "avg_ms": ms, "algorithmic_bytes": by, "achieved_GBs": gbs,
-                        "frac": gbs / peak if peak else None, "states": ent[0]["states"],
-                        "pair_and_D_bytes": 40.0 * ent[0]["states"]})
+    scan_states = float(sum(s.dim(u, d) for u, d in sectors))
+    kinds = {}
+    for e in log:
+        kinds.setdefault(e["states"], []).append(e)
+    per = []
+    for st_, ent in kinds.items():
+        if st_ == scan_states:
+            name = f"ground-state scan ({len(sectors)} sectors, {maxn} steps)"
+        elif st_ in [float(s.dim(u, d)) for u, d in sectors]:
+            name = "eigenvector pass (winning sector)"
+        else:
+            name = f"c / c^+ runs (excitation sectors, {maxn} steps)"
+        ms = sum(e["ms"] for e in ent) / len(ent)
+        by = sum(e["bytes"] for e in ent) / len(ent)
+        gbs = by / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+        per.append({"launch": name, "launches": len(ent), "avg_ms": ms, "algorithmic_bytes": by,
+                    "achieved_GBs": gbs, "frac": gbs / peak if peak else None, "states": st_,
+                    "pair_and_D_bytes": 40.0 * st_})
+    if per:
         roofline["per_launch"] = per
 
     hv = hv_leg(pkg, s, peak) if (world == 1 and not args.skip_hv) else None

@@ -53,7 +53,7 @@ EXPORTS = (
     "edzt_cluster_green_matrix", "edzt_gs_occupancy", "edzt_green_real", "edzt_server_create", "edzt_server_submit", "edzt_server_step", "edzt_server_result", "edzt_server_destroy",
     "edzt_server_cancel", "edzt_server_set_step_ms", "edzt_tune_sector", "edzt_clear_tuning",
     "edzt_instance_footprint", "edzt_set_fault_test", "edzt_diag_arpack",
-    "edzt_set_diag_solver", "edzt_hybridization", "edzt_local_green_bethe", "edzt_fit_bath", "edzt_dmft_bethe",
+    "edzt_set_diag_solver", "edzt_set_keep_vectors", "edzt_hybridization", "edzt_local_green_bethe", "edzt_fit_bath", "edzt_dmft_bethe",
 )
 # ground_state's diag_solver values (src/ground_state.f90:53-60).
 DIAG_LANCZOS = 1
@@ -194,6 +194,7 @@ def load_library(path: str = LIB_PATH):
     L.edzt_diag_lanczos.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _dp]
     L.edzt_diag_arpack.argtypes = [_vp, C.c_int, C.c_int, C.c_uint64, C.c_uint64, _dp, _vp, _vp, _vp, _ip]
     L.edzt_set_diag_solver.argtypes = [_vp, C.c_int]
+    L.edzt_set_keep_vectors.argtypes = [_vp, C.c_int]
     L.edzt_hybridization.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp]
     L.edzt_local_green_bethe.argtypes = [C.c_int, C.c_int, C.c_int, _vp, C.c_double, _vp, _vp, _vp]
     L.edzt_fit_bath.argtypes = [C.c_int] * 4 + [_vp] * 7 + [C.c_double, _vp]
@@ -458,6 +459,11 @@ class Solver:
     def set_diag_solver(self, diag_solver: int):
         """ground_state's diag_solver: DIAG_LANCZOS (1) or DIAG_ARPACK (2)."""
         self._check(self._L.edzt_set_diag_solver(self._h, int(diag_solver)))
+
+    def set_keep_vectors(self, keep: int):
+        """edzt_set_keep_vectors: 1 (default) keep the scan's Lanczos vectors
+        for the eigenvector when they fit, 0 rerun the recurrence."""
+        self._check(self._L.edzt_set_keep_vectors(self._h, int(keep)))
 
     def ground_state(self, sectors, maxnstep, seed=0, want_vec=True):
         sec = np.ascontiguousarray(np.asarray(sectors, dtype=np.int32).reshape(-1, 2))

@@ -189,6 +189,7 @@ struct edzt_ctx {
     std::string err;
     int engine = EDZT_ENGINE_FUSED;
     int diag_solver = EDZT_DIAG_LANCZOS;    // ground_state's diag_solver (ground_state.f90:53-60)
+    int keep_vectors = 1;                   // ground_state: keep the scan's Lanczos vectors when they fit
     ModelTables mt;                         // the model of the single-model entry points
     // bit strings and rank tables by (nsite, electron count): model-independent, shared
     std::map<std::pair<int, int>, std::unique_ptr<StrTable>> str_tables;
@@ -487,6 +488,7 @@ struct JobSpec {
     double* eig = nullptr;           // device, EIGVEC
     double* a = nullptr;             // device [maxnstep]
     double* b = nullptr;             // device [maxnstep]
+    double2* keep = nullptr;         // device [maxnstep + 1][dim]: keep every step's pair (else ping-pong)
     // results
     int nstep = 0;
     double norm0 = 0.0;
@@ -538,9 +540,15 @@ void run_jobs(edzt_ctx* c, std::vector<JobSpec>& specs, int force_wc = 0, int fo
         std::memset(&J, 0, sizeof(J));
         J.S = make_sector_mt(c, s.mt ? *s.mt : c->mt, s.nu, s.nd);
         const long long dim = J.S.dim;
-        for (int q = 0; q < 2; q++) {
-            bufs.emplace_back(c->pool, (size_t)dim);
-            J.YW[q] = bufs.back().p;
+        if (s.keep) {
+            J.keep = 1;
+            J.YW[0] = s.keep;
+            J.YW[1] = nullptr;
+        } else {
+            for (int q = 0; q < 2; q++) {
+                bufs.emplace_back(c->pool, (size_t)dim);
+                J.YW[q] = bufs.back().p;
+            }
         }
         dbufs.emplace_back(c->pool, (size_t)lz_d_size(J.S.up.count, J.S.dn.count));
         J.D = dbufs.back().p;
@@ -1015,6 +1023,19 @@ void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnste
         return;
     }
     std::vector<SectorResult> res(nsector);
+    // The scan keeps every step's (y, w) pairs when they fit in half of the
+    // free device memory: the winner's eigenvector is then one pass over its
+    // kept w_k instead of a second run of the recurrence (the same sum, in
+    // the same order, of the same vectors).
+    std::vector<Lease<double2>> kept(nsector);
+    bool keep = false;
+    if (c->engine == EDZT_ENGINE_FUSED && c->keep_vectors) {
+        long long states = 0;
+        for (int i = 0; i < nsector; i++) states += std::max(0LL, sector_dim(c, sectors[2 * i], sectors[2 * i + 1]));
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        keep = (double)states * (maxnstep + 1) * sizeof(double2) <= 0.5 * (double)free_b;
+    }
     if (c->engine == EDZT_ENGINE_FUSED) {
         std::vector<JobSpec> specs;
         std::vector<int> which;
@@ -1030,6 +1051,10 @@ void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnste
             s.maxnstep = maxnstep;
             s.a = ab.p + (size_t)(2 * i) * maxnstep;
             s.b = ab.p + (size_t)(2 * i + 1) * maxnstep;
+            if (keep) {
+                kept[i] = Lease<double2>(c->pool, (size_t)(maxnstep + 1) * sector_dim(c, nu, nd));
+                s.keep = kept[i].p;
+            }
             specs.push_back(s);
             which.push_back(i);
         }
@@ -1070,17 +1095,24 @@ void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnste
         CK(cudaMemcpyAsync(cf.p, r.coeff.data(), sizeof(double) * r.nstep, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(ab.p, r.a.data(), sizeof(double) * maxnstep, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(ab.p + maxnstep, r.b.data(), sizeof(double) * maxnstep, cudaMemcpyHostToDevice, c->stream));
-        std::vector<JobSpec> ev(1);
-        ev[0].nu = nu; ev[0].nd = nd;
-        ev[0].mode = LZ_EIGVEC;
-        ev[0].init = LZ_INIT_HASH;
-        ev[0].key = edzt_stream_key(seed, stream_of(best));
-        ev[0].maxnstep = r.nstep;
-        ev[0].coeff = cf.p;
-        ev[0].eig = c->gs_vec.p;
-        ev[0].a = ab.p;
-        ev[0].b = ab.p + maxnstep;
-        run_jobs(c, ev);
+        if (keep) {
+            launch_keep_combine(kept[best].p, dim, r.nstep, cf.p, c->gs_vec.p, c->stream);
+            c->launches += 1;
+            CKLAUNCH();
+        } else {
+            std::vector<JobSpec> ev(1);
+            ev[0].nu = nu; ev[0].nd = nd;
+            ev[0].mode = LZ_EIGVEC;
+            ev[0].init = LZ_INIT_HASH;
+            ev[0].key = edzt_stream_key(seed, stream_of(best));
+            ev[0].maxnstep = r.nstep;
+            ev[0].coeff = cf.p;
+            ev[0].eig = c->gs_vec.p;
+            ev[0].a = ab.p;
+            ev[0].b = ab.p + maxnstep;
+            run_jobs(c, ev);
+        }
+        for (auto& k : kept) k = Lease<double2>();
         DevSector S = make_sector(c, nu, nd);
         c->gs_residual = finish_eigvec(c, S, c->gs_vec.p, r.e);
         c->gs_up = nu; c->gs_dn = nd; c->gs_isector = best; c->gs_e0 = r.e;
@@ -2459,6 +2491,14 @@ int edzt_set_diag_solver(edzt_ctx* c, int diag_solver)
         if (diag_solver != EDZT_DIAG_LANCZOS && diag_solver != EDZT_DIAG_ARPACK)
             throw EdztError{EDZT_ERR_ARG, "invalid diag solver"};
         c->diag_solver = diag_solver;
+    });
+}
+
+int edzt_set_keep_vectors(edzt_ctx* c, int keep)
+{
+    return guarded(c, [&] {
+        if (keep != 0 && keep != 1) throw EdztError{EDZT_ERR_ARG, "keep must be 0 or 1"};
+        c->keep_vectors = keep;
     });
 }
 

@@ -44,6 +44,11 @@ void launch_build_spin_ops(const DevModel& m, int sigma, int count, const uint32
 int edzt_max_hops(const DevModel& m, int sigma, int n);
 
 // ---- kernels.cu: standalone (non-persistent) kernels ------------------------
+// Ground-state vector from the kept pairs of a coefficient run: out =
+// sum_{k=1..nstep} coeff[k-1] w_k, w_k the second value of step k's pair,
+// accumulated in step order as the eigenvector pass does.
+void launch_keep_combine(const double2* keep, long long dim, int nstep, const double* coeff, double* out,
+                         cudaStream_t s);
 // H.v in two phases (hv_phase.cuh); scratch: hx_scratch_size doubles of
 // device memory (the down-hop part, slab-major, slabs of up to 16 columns).
 void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, double* scratch, cudaStream_t s);
@@ -131,7 +136,7 @@ struct LzState {
 // 16-byte access each: step k writes YW[k & 1] and reads YW[(k - 1) & 1].
 struct LzJob {
     DevSector S;
-    double2* YW[2];       // ping-pong pair buffers [dim]
+    double2* YW[2];       // ping-pong pair buffers [dim]; keep: YW[0] holds every step's pair, step k at k * dim
     double* D;            // [lz_d_size] down-hop part of H v_k, column phase -> row phase, slab-major:
                           // the slab of columns [c0, c0 + WC) is the block [ndn][WC] at c0 * ndn
     double* eig;          // EIGVEC: output eigenvector (unnormalised)
@@ -141,13 +146,19 @@ struct LzJob {
     int maxnstep;         // COEFF: LanczosSteps; EIGVEC: nstep of the coefficient pass
     int mode;
     int init;
-    int pad;
+    int keep;             // 1: the pairs of every step are kept ([maxnstep + 1][dim] at YW[0])
     LzPhase ph[2];
     LzState* st;          // [2] the run's state by phase parity (kept across launches of a sliced run)
     uint64_t key;         // LZ_INIT_HASH
     ApplyCArgs ac;        // LZ_INIT_APPLYC
     const double* src;    // LZ_INIT_APPLYC: the ground state; LZ_INIT_COPY: the start vector
 };
+
+// The pair buffer step k of a run writes (and step k + 1 reads).
+__host__ __device__ inline double2* lz_pairs(const LzJob& J, int k)
+{
+    return J.keep ? J.YW[0] + (long long)k * J.S.dim : J.YW[k & 1];
+}
 
 // Doubles of a job's D buffer (slabs of up to 8 columns).
 inline long long lz_d_size(int nup, int ndn) { return (long long)((nup + 7) / 8) * 8 * ndn; }
@@ -184,7 +195,8 @@ size_t lz_sync_bytes(int G);
 // Tile shapes of the jobs of one launch: every job's rows per tile and
 // columns per slab (a nonzero jobs[j].ph[].width on entry is a preset, kept
 // when it fits), the launch's block size (prefer_block 512: one CTA of 512
-// threads per SM even when two of 256 would fit), grid and shared memory;
+// threads per SM; 256: two of 256 whenever they fit; 0: two of 256 unless a
+// job has long lines or needs more shared memory), grid and shared memory;
 // the phases' tile lists, participants and slots are filled in.  prefix
 // receives, per phase, the jobs' first tiles [njobs + 1], then per phase
 // every CTA's first tile [grid + 1] (CTA b takes the contiguous tiles

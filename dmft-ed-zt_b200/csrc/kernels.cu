@@ -1,6 +1,7 @@
 // kernels.cu — standalone (one launch per operation) sm_100a kernels:
 // H.v, the BLAS-1 steps of the plain Lanczos drop-in, apply_c and the
 // continued fractions.  The fused persistent Lanczos lives in lanczos.cu.
+#include <algorithm>
 #include <cuda_runtime.h>
 #include "edzt_internal.h"
 #include "hv_phase.cuh"
@@ -205,6 +206,33 @@ void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, d
         default: launch_hx_row<1, kHxThreads>(S, x, scratch, wc, y, accumulate, s); break;
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Ground-state vector from kept Lanczos pairs (the eigenvector pass's sum,
+// src/lanczos_solver.f90:213-300, without rerunning the recurrence).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_keep_combine(const double2* __restrict__ keep, long long dim, int nstep,
+                                                      const double* __restrict__ coeff, double* __restrict__ out)
+{
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < dim; e += (long long)gridDim.x * blockDim.x) {
+        const double* w = reinterpret_cast<const double*>(keep + dim + e) + 1;   // w_1
+        double acc = __ldg(coeff) * __ldcs(w);
+#pragma unroll 8
+        for (int k = 2; k <= nstep; k++) acc = fma(__ldg(coeff + k - 1), __ldcs(w + 2 * (k - 1) * dim), acc);
+        out[e] = acc;
+    }
+}
+
+void launch_keep_combine(const double2* keep, long long dim, int nstep, const double* coeff, double* out,
+                         cudaStream_t s)
+{
+    if (dim <= 0 || nstep <= 0) return;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long blocks = std::min<long long>((dim + 255) / 256, 8LL * nsm);
+    k_keep_combine<<<(unsigned)blocks, 256, 0, s>>>(keep, dim, nstep, coeff, out);
 }
 
 // ---------------------------------------------------------------------------

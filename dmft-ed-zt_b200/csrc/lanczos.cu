@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
         constexpr int WC = decltype(wc_tag)::value;
         constexpr int WS = phase_stride(WC);
         const int nup = sJ.S.up.count, ndn = sJ.S.dn.count, k = sS.k;
-        const double2* __restrict__ pin = sJ.YW[(k + 1) & 1];
+        const double2* __restrict__ pin = lz_pairs(sJ, k - 1);
         const double am = -sS.a_prev;
         const int c0 = tl * WC;
         double* ws = chunk;
@@ -364,8 +364,8 @@ __global__ void __launch_bounds__(512) k_lanczos(LzBatch B, const LzJob* __restr
         constexpr int R = decltype(r_tag)::value;
         constexpr int RS = phase_stride(R);
         const int nup = sJ.S.up.count, ndn = sJ.S.dn.count, k = sS.k;
-        const double2* __restrict__ pin = sJ.YW[(k + 1) & 1];
-        double2* __restrict__ pout = sJ.YW[k & 1];
+        const double2* __restrict__ pin = lz_pairs(sJ, k - 1);
+        double2* __restrict__ pout = lz_pairs(sJ, k);
         const double am = -sS.a_prev, bk = sS.b_cur, rb = 1.0 / bk, n0 = sS.norm0;
         const bool first = (k == 1);
         const bool coeff = (sJ.mode == LZ_COEFF);
@@ -529,6 +529,7 @@ cudaError_t launch_lanczos_persistent(const LzBatch& B, const LzJob* jobs, const
 // Per-CTA dynamic shared memory: two CTAs of 256 threads per SM when every
 // job fits, else one CTA of 512 threads per SM.
 static constexpr size_t kLzSmemTwoPerSm = 108 * 1024;
+static constexpr int kLzLongLine = 1500;
 // Fixed cost of a tile in states, for cutting the tile list into CTA ranges
 static constexpr double kLzTileCost = 1024.0;
 
@@ -560,12 +561,19 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, 
     const size_t fixed = lz_fixed_smem();
     size_t need_min = 0;
     long long lines8 = 0;
+    int longest = 0;
     for (int j = 0; j < nj; j++) {
         const int nup = jobs[j].S.up.count, ndn = jobs[j].S.dn.count;
         need_min = std::max(need_min, std::max(lz_row_smem(nup, 1), lz_col_smem(ndn, 2)));
         lines8 += (ndn + 7) / 8 + (nup + 15) / 16;
+        longest = std::max(longest, std::max(nup, ndn));
     }
-    const bool two = fixed + need_min <= kLzSmemTwoPerSm && prefer_block != 512;
+    // Lines of kLzLongLine strings or more (nsite >= 13 near half filling)
+    // run faster as one 512-thread CTA per SM with twice the shared memory
+    // for wider tiles (measured with the tuner: 5-35% per step at nsite
+    // 13-15, equal at 16); shorter lines as two 256-thread CTAs.
+    const bool two = fixed + need_min <= kLzSmemTwoPerSm &&
+                     (prefer_block == 256 || (longest < kLzLongLine && prefer_block != 512));
     P.block = two ? 256 : 512;
     const size_t budget = (two ? kLzSmemTwoPerSm : kLzSmemMax) - fixed;
     const int G_est = (two ? 2 : 1) * nsm;

@@ -84,6 +84,11 @@ module edzt_iface
       type(c_ptr), value :: ctx
       integer(c_int), value :: diag_solver                    ! 1 Lanczos, 2 ARPACK
     end function
+    integer(c_int) function edzt_set_keep_vectors(ctx, keep) bind(C, name="edzt_set_keep_vectors")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: keep                           ! 1 keep when they fit, 0 rerun
+    end function
     integer(c_int) function edzt_ground_state(ctx, nsector, sectors, maxnstep, seed, isector, e0, gsvec, &
         e_sector) bind(C, name="edzt_ground_state")
       import :: c_int, c_ptr, c_double, c_int64_t

@@ -154,13 +154,24 @@ int edzt_diag_arpack(edzt_ctx *ctx, int ne_up, int ne_dn, uint64_t seed, uint64_
 #define EDZT_DIAG_ARPACK 2
 int edzt_set_diag_solver(edzt_ctx *ctx, int diag_solver);
 
+/* Whether ground_state's fused scan keeps every step's Lanczos vectors for
+ * the eigenvector (edzt_ground_state): 1 (default) when they fit in half of
+ * the free device memory, 0 never (the winner's recurrence is run again, as
+ * src/lanczos_solver.f90:213-300 does).  Anything else EDZT_ERR_ARG. */
+int edzt_set_keep_vectors(edzt_ctx *ctx, int keep);
+
 /* ground_state (src/ground_state.f90:1-81): scans sectors[nsector][2] =
  * (ne_up, ne_dn), keeps the lowest energy (a later sector wins only if lower
  * by more than 1e-10*max(1,|E|)), and keeps its normalised vector resident
  * on the device for edzt_cluster_green_ftn.  Sector i starts Lanczos from
  * stream i of `seed`.  gsvec (nullable, host or device) receives the vector
  * (gs%vec, src/eigpair.f90:5-9); e_sector (nullable) [nsector] the per-sector
- * lowest energies. */
+ * lowest energies.  Device memory: when (maxnstep + 1) * 16 bytes per state
+ * of all sectors fit in half of the free device memory, the scan keeps every
+ * step's Lanczos vectors and the ground-state vector is their sum (one pass);
+ * otherwise the winner's recurrence is run again, as the reference's
+ * lanczos_ground_state does.  Both form the same sum; the rerun sums
+ * ||v_init|| again, so the two agree to rounding. */
 int edzt_ground_state(edzt_ctx *ctx, int nsector, const int *sectors, int maxnstep, uint64_t seed,
                       int *isector, double *e0, double *gsvec, double *e_sector);
 

@@ -91,6 +91,33 @@ def test_diag_lanczos(pkg, solver, oracle_mod):
     assert abs(abs(r["vec"] @ ref["vec"]) - 1.0) < 1e-8
 
 
+def test_ground_state_vector_from_kept_pairs_matches_rerun(pkg, solver):
+    """ground_state takes the eigenvector from the scan's kept Lanczos pairs
+    (they fit in memory here) or, with keeping switched off, reruns the
+    winner's recurrence (src/lanczos_solver.f90:213-300): the same sector and
+    E0, the same vector to rounding, the same G."""
+    rng = np.random.default_rng(77)
+    m = random_model(pkg, rng, 1, 11)                     # nsite 12
+    solver.set_model(m)
+    sectors = [(5, 6), (6, 6), (6, 5)]
+    omega = pkg.matsubara(64, 50.0)
+    kept = solver.ground_state(sectors, 200, seed=5)
+    gk = solver.cluster_green_ftn(1, 200, omega)["G_cl"]
+    try:
+        solver.set_keep_vectors(0)
+        rerun = solver.ground_state(sectors, 200, seed=5)
+        gr = solver.cluster_green_ftn(1, 200, omega)["G_cl"]
+    finally:
+        solver.set_keep_vectors(1)
+    assert kept["isector"] == rerun["isector"]
+    assert abs(kept["e0"] - rerun["e0"]) <= 1e-12 * max(1.0, abs(rerun["e0"]))
+    assert abs(abs(kept["vec"] @ rerun["vec"]) - 1.0) <= 1e-12
+    assert np.abs(np.abs(kept["vec"]) - np.abs(rerun["vec"])).max() <= 1e-10
+    assert np.abs(gk - gr).max() <= 1e-10
+    with pytest.raises(pkg.EDError):
+        solver.set_keep_vectors(2)
+
+
 @pytest.fixture(scope="module")
 def bethe(configs, oracle_mod):
     cfg = configs.bethe_n6()
