@@ -699,7 +699,8 @@ def run_gpu(args):
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
                 "config": config_dict(cfg, world),
                 "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)),
-                               "p99": float(np.percentile(lat_sorted, 99))},
+                               "p99": float(np.percentile(lat_sorted, 99)),
+                               "each": [round(float(x), 3) for x in lat]},
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
                 "plain_gpu": plain, "hv": hv, "batched": batched, "served": served, "clocks": clk, "e0": e0.value}
         print(json.dumps(line))

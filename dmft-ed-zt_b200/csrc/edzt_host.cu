@@ -190,6 +190,7 @@ struct edzt_ctx {
     int engine = EDZT_ENGINE_FUSED;
     int diag_solver = EDZT_DIAG_LANCZOS;    // ground_state's diag_solver (ground_state.f90:53-60)
     int keep_vectors = 1;                   // ground_state: keep the scan's Lanczos vectors when they fit
+    size_t free_at_create = 0;              // free device memory when the context was created
     ModelTables mt;                         // the model of the single-model entry points
     // bit strings and rank tables by (nsite, electron count): model-independent, shared
     std::map<std::pair<int, int>, std::unique_ptr<StrTable>> str_tables;
@@ -1024,17 +1025,17 @@ void ground_state_impl(edzt_ctx* c, int nsector, const int* sectors, int maxnste
     }
     std::vector<SectorResult> res(nsector);
     // The scan keeps every step's (y, w) pairs when they fit in half of the
-    // free device memory: the winner's eigenvector is then one pass over its
-    // kept w_k instead of a second run of the recurrence (the same sum, in
-    // the same order, of the same vectors).
+    // device memory that was free when the context was created (queried once:
+    // a query per solve can wait on the driver behind other processes'
+    // queries): the winner's eigenvector is then one pass over its kept w_k
+    // instead of a second run of the recurrence (the same sum, in the same
+    // order, of the same vectors).  The pool keeps the blocks for the next solve.
     std::vector<Lease<double2>> kept(nsector);
     bool keep = false;
     if (c->engine == EDZT_ENGINE_FUSED && c->keep_vectors) {
         long long states = 0;
         for (int i = 0; i < nsector; i++) states += std::max(0LL, sector_dim(c, sectors[2 * i], sectors[2 * i + 1]));
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
-        keep = (double)states * (maxnstep + 1) * sizeof(double2) <= 0.5 * (double)free_b;
+        keep = (double)states * (maxnstep + 1) * sizeof(double2) <= 0.5 * (double)c->free_at_create;
     }
     if (c->engine == EDZT_ENGINE_FUSED) {
         std::vector<JobSpec> specs;
@@ -2223,6 +2224,8 @@ int edzt_ctx_create(int device, edzt_ctx** out)
         CK(cudaMallocHost((void**)&c->pinned, sizeof(double) * 32));
         CK(cudaEventCreate(&c->ev0));
         CK(cudaEventCreate(&c->ev1));
+        size_t total_b = 0;
+        CK(cudaMemGetInfo(&c->free_at_create, &total_b));
     });
     if (rc != EDZT_OK) {
         edzt_ctx_destroy(c);

@@ -23,13 +23,18 @@
 // Every neighbour value comes from shared memory, every global access is a
 // coalesced stream (pair buffers, D, the eigenvector), and both reductions
 // are exact sums, as in the reference.  The tiles of all jobs of a phase
-// form one list; CTA b takes tiles b, b+G, ... in every phase, and each
-// job's participants in a phase write one partial sum each into their slot
-// (double-buffered by step parity).  Every participating CTA re-derives a
-// job's scalars from the slots in a fixed order, so all of them get the same
-// bits; the first participant also stores them.
+// form one list, cut into one contiguous range per CTA at equal modelled
+// cost (lz_plan); within a job the column slabs are numbered by round, so
+// the CTAs stage neighbouring slabs at the same time.  A job's participants
+// in a phase (the CTAs whose range meets its tiles) write one partial sum
+// each into their slot (double-buffered by step parity).  Every
+// participating CTA re-derives a job's scalars from the slots in a fixed
+// order, so all of them get the same bits; the first participant also
+// stores them.
 //
-// The eigenvector pass (LZ_EIGVEC) reruns the recurrence with the stored
+// The pairs of a run are ping-pong buffers, or (LzJob::keep) one slot per
+// step, so that the eigenvector can be summed from them afterwards.  The
+// eigenvector pass (LZ_EIGVEC) instead reruns the recurrence with the stored
 // a, b (src/lanczos_solver.f90:213-300) and accumulates sum_k coeff_k w_k.
 //
 // A launch may be a slice of longer runs (LzBatch::slice): when its phase

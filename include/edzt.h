@@ -156,7 +156,7 @@ int edzt_set_diag_solver(edzt_ctx *ctx, int diag_solver);
 
 /* Whether ground_state's fused scan keeps every step's Lanczos vectors for
  * the eigenvector (edzt_ground_state): 1 (default) when they fit in half of
- * the free device memory, 0 never (the winner's recurrence is run again, as
+ * the device memory free at context creation, 0 never (the winner's recurrence is run again, as
  * src/lanczos_solver.f90:213-300 does).  Anything else EDZT_ERR_ARG. */
 int edzt_set_keep_vectors(edzt_ctx *ctx, int keep);
 
@@ -167,7 +167,8 @@ int edzt_set_keep_vectors(edzt_ctx *ctx, int keep);
  * stream i of `seed`.  gsvec (nullable, host or device) receives the vector
  * (gs%vec, src/eigpair.f90:5-9); e_sector (nullable) [nsector] the per-sector
  * lowest energies.  Device memory: when (maxnstep + 1) * 16 bytes per state
- * of all sectors fit in half of the free device memory, the scan keeps every
+ * of all sectors fit in half of the device memory that was free when the
+ * context was created, the scan keeps every
  * step's Lanczos vectors and the ground-state vector is their sum (one pass);
  * otherwise the winner's recurrence is run again, as the reference's
  * lanczos_ground_state does.  Both form the same sum; the rerun sums
