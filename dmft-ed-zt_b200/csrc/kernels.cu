@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include "edzt_internal.h"
 #include "hv_phase.cuh"
+#include "hv_gather.cuh"
 
 static constexpr int kWintDoubles = EDZT_MAX_P * EDZT_MAX_P;
 static constexpr int kAmpDoubles = EDZT_MAX_AMP;
@@ -27,6 +28,7 @@ int kernels_debug_bad(long long* out4)
 static constexpr int kHxThreads = 256;
 static constexpr int kHxThreadsLong = 1024;          // lines of kHxLongLine strings or more
 static constexpr int kHxLongLine = 1500;
+static constexpr int kHxGatherLine = 3000;            // single-pass form from here (nsite >= 14 near half filling)
 static constexpr size_t kHxSmemSoft = 100 * 1024;    // two CTAs per SM
 static constexpr size_t kHxSmemHard = 210 * 1024;    // one CTA per SM
 
@@ -174,10 +176,82 @@ static void launch_hx_col(const DevSector& S, const double* x, double* D, cudaSt
     k_hx_col<W, NT><<<slabs, NT, sm, s>>>(S, x, D);
 }
 
+// ---------------------------------------------------------------------------
+// Single-pass H.v for long lines (hv_gather.cuh): one CTA per tile of R full
+// rows staged in shared memory with their down-hop records; the up hops read
+// the staged rows, the down hops gather coalesced slices of other rows from
+// global memory.  T threads per CTA, 64 registers (32 warps per SM).
+// ---------------------------------------------------------------------------
+static constexpr size_t kGatherTileBytes = 24 * 1024;
+
+template <bool ACC, int T>
+__global__ void __launch_bounds__(T, T == 512 ? 2 : 1) k_hx_gather(DevSector S, const double* __restrict__ x,
+                                                                  double* __restrict__ y, int R)
+{
+    extern __shared__ __align__(16) double smem[];
+    double* wint = smem;
+    double* amp = smem + kWintDoubles;
+    const int nup = S.up.count, ndn = S.dn.count;
+    Chunk C = chunk_layout(smem + kWintDoubles + kAmpDoubles, R, nup, S.dn.hw);
+    const int r0 = blockIdx.x * R;
+    const int rows = min(R, ndn - r0);
+    const int n = rows * nup;
+    const long long g0 = (long long)r0 * nup;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) C.xs[e] = __ldg(x + g0 + e);
+    stage_rows(S.dn, C, r0, rows);
+    stage_table(S.wint, S.P * S.P, wint);
+    stage_table(S.up.amp, S.up.namp, amp);
+    __syncthreads();
+    auto fetch = [&](long long idx) {
+        EDZT_OK_OR(idx >= 0 && idx < S.dim, 61, idx, S.dim, blockIdx.x, return 0.0)
+        return __ldg(x + idx);
+    };
+    const SrcVec src{x};
+    int r = threadIdx.x / nup, iu = threadIdx.x - r * nup;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        double du, dn;
+        hv_elem(S, C, wint, amp, src, r, iu, C.xs[e], du, dn);
+        double acc = du + dn;
+        if (S.has_j) acc = hv_exchange(S, C, r, iu, acc, fetch);
+        const long long g = g0 + e;
+        y[g] = ACC ? y[g] + acc : acc;
+        iu += blockDim.x;
+        while (iu >= nup) { iu -= nup; ++r; }
+    }
+}
+
+template <int T>
+static void launch_hx_gather(const DevSector& S, const double* x, double* y, int accumulate, cudaStream_t s)
+{
+    static std::atomic<unsigned long long> attr_set{0};
+    if (edzt_once_per_device(attr_set)) {
+        cudaFuncSetAttribute(k_hx_gather<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
+        cudaFuncSetAttribute(k_hx_gather<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHxSmemHard);
+    }
+    const int nup = S.up.count, ndn = S.dn.count;
+    const size_t row = staged_row_bytes(nup, S.dn.hw);
+    const int R = std::max(1, std::min(ndn, (int)(kGatherTileBytes / row)));
+    const int tiles = (ndn + R - 1) / R;
+    const size_t smem = (kWintDoubles + kAmpDoubles) * sizeof(double) + (size_t)R * row;
+    if (accumulate) k_hx_gather<true, T><<<tiles, T, smem, s>>>(S, x, y, R);
+    else k_hx_gather<false, T><<<tiles, T, smem, s>>>(S, x, y, R);
+}
+
+// Whether H.v of a sector takes the single-pass form: lines of
+// kHxGatherLine strings or more (measured faster there: the two-phase
+// slabs and tiles are too narrow).
+bool hx_single_pass(int nup, int ndn) { return std::max(nup, ndn) >= kHxGatherLine; }
+
 void launch_hx(const DevSector& S, const double* x, double* y, int accumulate, double* scratch, cudaStream_t s)
 {
     const int nup = S.up.count, ndn = S.dn.count;
     if (nup <= 0 || ndn <= 0) return;
+    if (hx_single_pass(nup, ndn)) {
+        // 1024 threads from 32 M states, else 512 (two CTAs per SM)
+        if (S.dim >= (32LL << 20)) launch_hx_gather<1024>(S, x, y, accumulate, s);
+        else launch_hx_gather<512>(S, x, y, accumulate, s);
+        return;
+    }
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
