@@ -210,6 +210,11 @@ struct LzPlan {
     long long slots = 0;
 };
 LzPlan lz_plan(int device, LzJob* jobs, int njobs, std::vector<long long>& prefix, int prefer_block = 0);
+// The device-free part of lz_plan: given every job's widths (ph[].width) and
+// the grid G, the phases' tile lists, CTA ranges, participants and the column
+// phase's slab order (prefix as lz_plan describes it), the tiles per phase
+// (total) and the number of partial-sum slots (returned).
+long long lz_cut(LzJob* jobs, int njobs, int G, std::vector<long long>& prefix, long long total[2]);
 
 // ---- edzt_host.cu: context accessors (no table building, no allocation) -----
 struct edzt_ctx;

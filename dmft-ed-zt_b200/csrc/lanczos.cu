@@ -599,7 +599,13 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, 
     P.smem = fixed + chunk;
     P.grid = lz_grid_size(device, P.smem, P.block);
     if (P.grid <= 0) return P;
-    const int G = P.grid;
+    P.slots = lz_cut(jobs, nj, P.grid, prefix, P.total);
+    return P;
+}
+
+long long lz_cut(LzJob* jobs, int nj, int G, std::vector<long long>& prefix, long long total[2])
+{
+    long long slots = 0;
     prefix.assign(2 * (size_t)(nj + 1) + 2 * (size_t)(G + 1), 0);
     std::vector<long long> slab_order;
     for (int ph = 0; ph < 2; ph++) {
@@ -612,7 +618,7 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, 
             pre[j + 1] = pre[j] + Q.ntiles;
         }
         const long long T = pre[nj];
-        P.total[ph] = T;
+        total[ph] = T;
         // CTA ranges: with no more tiles than CTAs, CTA b takes tile b; else
         // the list is cut where the running cost crosses b/G of the total
         // (a tile costs its states plus a fixed amount for its staging round
@@ -649,8 +655,8 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, 
             LzPhase& Q = jobs[j].ph[ph];
             Q.part0 = owner(Q.tile0);
             Q.npart = owner(Q.tile0 + Q.ntiles - 1) - Q.part0 + 1;
-            Q.slot0 = P.slots;
-            P.slots += Q.npart;
+            Q.slot0 = slots;
+            slots += Q.npart;
         }
         // Column phase: the slab each tile position stages.  A participant
         // takes its positions in order; numbering the slabs by round (the
@@ -672,5 +678,5 @@ LzPlan lz_plan(int device, LzJob* jobs, int nj, std::vector<long long>& prefix, 
         }
     }
     prefix.insert(prefix.end(), slab_order.begin(), slab_order.end());
-    return P;
+    return slots;
 }
